@@ -1,0 +1,357 @@
+"""Benchmark of the fault-stiffness build on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config h50]
+
+Workload (default `h50`): the BP8 grid at h = 50 m, L_fault = 800 m,
+L_normal = 400 m (33 x 33 x 9 nodes per side, 58,806 DOF), Omega_f = the whole
+fault plane (l_f = L_fault), i.e. all 2,178 unit-slip columns of K. One step =
+one build of those K columns by batched mixed-precision CG (FP32 stencil and
+vector updates, FP64 reliable updates, rtol 1e-10 on the FP64 true residual),
+traction extraction included. Inputs are unit slips (synthetic by
+definition; no dataset is involved).
+
+Prints one JSON line (rank 0). `value` = K columns/s with K written to
+device memory; `e2e` = the same through the public host API (`fault_stiffness`
+into a host array, every step). Under torchrun (N > 1) each rank builds a
+contiguous shard of the columns on its own GPU (no collective on the data
+path); the step time is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "K columns/s at K rel err <=1e-8 (batched mixed-precision CG vs plain FP64 CG); solve p99 ms"
+CONFIGS = {
+    # name: dz, L_fault, L_normal, l_f
+    "h100": (100.0, 800.0, 800.0, 800.0),   # 17x17x9 (the reference's 17x17x5 case needs >= 9 normal nodes)
+    "h50": (50.0, 800.0, 400.0, 800.0),     # 33x33x9, 2,178 columns
+    "h20": (20.0, 800.0, 400.0, 800.0),     # 81x81x21, 13,122 columns
+}
+MU = 32.04e9
+NU = 0.25
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="h50")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(cfg):
+    dz, Lf, Ln, lf = CONFIGS[cfg]
+    n1 = int(round(Ln / dz)) + 1
+    n23 = int(round(2 * Lf / dz)) + 1
+    nf = (int(round(2 * lf / dz)) + 1) ** 2
+    return (f"bp8 fault stiffness h={dz:g}m L_fault={Lf:g} L_normal={Ln:g} l_f={lf:g}: "
+            f"{n23}x{n23}x{n1} nodes/side ({6 * n1 * n23 * n23} DOF), {2 * nf} unit-slip columns"), n1, n23, nf
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier_max(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_port_sample(cfg, ncols_sample, seed=0, threads=0):
+    """The oracle's C restatement of the reference column loop (assembled CSR
+    A, FP64 CG, Krylov rule), all host threads, on a seeded column sample."""
+    from oracle.fault import FaultElasticity as OFE, bp8_grids, lame_lambda
+    from oracle.cref import CRefStiffness, max_threads
+    dz, Lf, Ln, lf = CONFIGS[cfg]
+    gm, gp = bp8_grids(dz, Lf, Ln)
+    ofe = OFE(gm, gp, lame_lambda(MU, NU), MU, lf)
+    ref = CRefStiffness(ofe)
+    rng = np.random.default_rng(seed)
+    cols = np.sort(rng.choice(2 * ofe.nf, size=min(ncols_sample, 2 * ofe.nf), replace=False))
+    nt = threads if threads > 0 else max_threads()
+    return ofe, ref, cols, nt
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    wl, n1, n23, nf = workload_name(args.config)
+    ofe, ref, cols, nt = cpu_port_sample(args.config, 64 if args.config != "h20" else 8)
+    for _ in range(args.warmup):
+        ref.columns(cols[: max(1, len(cols) // 8)], nthreads=nt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, it, ok = ref.columns(cols, nthreads=nt)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = len(cols) / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "columns/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (unit slips)",
+        "config": {"workload": wl, "sample_columns": int(len(cols)), "mean_iterations": float(np.mean(it))},
+        "cpu_baseline": {"value": v, "unit": "columns/s", "cores": nt, "kind": "port",
+                         "sample": f"{len(cols)} seeded columns of the workload per step (C restatement of the "
+                                   "reference column loop, assembled CSR A, FP64 Krylov-rule CG, OpenMP over columns)"},
+        "e2e": {"value": v, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    world, rank, local = dist_init(args)
+    from __graft_entry__ import import_package
+    eqd = import_package()
+    import torch
+
+    dz, Lf, Ln, lf = CONFIGS[args.config]
+    wl, n1, n23, nf = workload_name(args.config)
+    ncols = 2 * nf
+    lo, hi = ncols * rank // world, ncols * (rank + 1) // world
+    cols = np.arange(lo, hi, dtype=np.int32)
+    g = eqd.bp8_grids(dz, Lf, Ln)
+    fe = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="mixed")
+    lib = eqd._abi.lib()
+    opts = fe.rs.opts()
+    opts.itmax = 20000  # safety cap (a converging column needs a few hundred)
+    kdev = torch.empty((len(cols), 2 * nf), dtype=torch.float64, device=f"cuda:{local}")
+
+    def device_step():
+        st = eqd._abi.Stats()
+        eqd._abi.check(lib.eqd_stiffness_columns_device(
+            fe.handle, eqd._abi.ptr(cols), C.c_int32(len(cols)), C.byref(opts),
+            C.c_void_p(kdev.data_ptr()), None, None, C.byref(st)))
+        return st
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    dev_s, launches, step_ms, iters = [], 0, [], 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = device_step()
+        dev_s.append(st.device_seconds)
+        step_ms.append(st.device_seconds * 1e3)
+        launches += st.kernel_launches
+        iters += st.iterations
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = clk.stop()
+    barrier(world)
+    dev_total = barrier_max(world, float(sum(dev_s)))
+    ms_per_step = dev_total / args.steps * 1e3
+    value = ncols / (dev_total / args.steps)
+    mean_it = iters / (args.steps * len(cols))
+
+    # End to end through the public API: host K every step.
+    for _ in range(1):
+        Kh = eqd.stiffness_columns(fe, cols)[0]
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        Kh, it_h, st_h = eqd.stiffness_columns(fe, cols)
+    e2e_dt = barrier_max(world, (time.perf_counter() - t0) / e2e_steps)
+    e2e = {"value": ncols / e2e_dt, "unit": "columns/s", "h2d_bytes_per_step": int(len(cols) * 4 * 3),
+           "d2h_bytes_per_step": int(len(cols) * 2 * nf * 8 + len(cols) * 5)}
+
+    if rank != 0:
+        return
+
+    # Accuracy of this K against a tight FP64 solve of the same columns (GPU
+    # plain FP64 CG, rtol 1e-12) and against the CPU oracle on a column sample.
+    Kmix = kdev.cpu().numpy().T
+    fe64 = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64", rtol=1e-12)
+    K64 = eqd.stiffness_columns(fe64, cols)[0]
+    k_err = float(np.linalg.norm(Kmix - K64) / np.linalg.norm(K64))
+    k_max = float(abs(Kmix - K64).max() / abs(K64).max())
+
+    # Plain FP64 CG, one right-hand side at a time (the comparator).
+    plain = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64", chunk=1)
+    rng = np.random.default_rng(1)
+    sample = np.sort(rng.choice(ncols, size=min(24, ncols), replace=False)).astype(np.int32)
+    eqd.stiffness_columns(plain, sample[:2])
+    t0 = time.perf_counter()
+    lat = []
+    for c in sample:
+        t1 = time.perf_counter()
+        eqd.stiffness_columns(plain, [c])
+        lat.append((time.perf_counter() - t1) * 1e3)
+    plain_v = len(sample) / (time.perf_counter() - t0)
+    # Batched FP64 (same path, all columns) for context.
+    b64 = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64")
+    eqd.stiffness_columns(b64, cols[:64])
+    st64 = eqd._abi.Stats()
+    eqd._abi.check(lib.eqd_stiffness_columns_device(
+        b64.handle, eqd._abi.ptr(cols), C.c_int32(len(cols)), C.byref(b64.rs.opts()),
+        C.c_void_p(kdev.data_ptr()), None, None, C.byref(st64)))
+    batched64_v = len(cols) / st64.device_seconds
+
+    # Roofline of the dominant kernel: FP32 stencil apply over the batch.
+    ms = C.c_double()
+    by = C.c_double()
+    eqd._abi.check(lib.eqd_profile_apply(fe.handle, C.c_int32(len(cols)), C.c_int32(eqd._abi.EQD_PREC_MIXED),
+                                         C.c_int32(3), C.c_int32(10), C.byref(ms), C.byref(by)))
+    achieved = by.value / (ms.value * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "apply_traffic.json")
+    if os.path.exists(tp):
+        t = json.load(open(tp)).get(args.config)
+        if t:
+            traffic = t["dram_bytes_per_launch_per_column"] * len(cols)
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        ofe, ref, ccols, nt = cpu_port_sample(args.config, 256 if args.config != "h20" else 8)
+        Kc, itc, okc = ref.columns(ccols[:8], nthreads=nt, rtol=1e-13)
+        o_err = float(np.linalg.norm(Kmix[:, ccols[:8]] - Kc) / np.linalg.norm(Kc))
+        t0 = time.perf_counter()
+        ref.columns(ccols, nthreads=nt)
+        cdt = time.perf_counter() - t0
+        cpu = {"value": len(ccols) / cdt, "unit": "columns/s", "cores": nt, "kind": "port",
+               "sample": f"{len(ccols)} seeded columns of the workload, rtol 1e-10, OpenMP over columns "
+                         "(C restatement of the reference column loop on the assembled CSR A)",
+               "k_rel_err_vs_oracle_sample": o_err}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (unit slips; the workload is fully "
+                                                          "determined by the grid)",
+        "config": {"workload": wl, "columns": ncols, "precision": "mixed (FP32 CG, FP64 reliable updates)",
+                   "rtol": opts.rtol, "parallelism": f"column shards x{world}",
+                   "l2": "inputs larger than L2 (working set %.1f GB)" % (len(cols) * 59400 * 24 / 1e9
+                                                                         if args.config == "h50" else 0),
+                   "mean_iterations": mean_it},
+        "k_rel_err": {"frobenius_vs_fp64_rtol1e-12": k_err, "max_entry_vs_fp64_rtol1e-12": k_max},
+        "solve_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                     "what": "whole-batch build time per step"},
+        "plain_fp64_single_rhs": {"value": plain_v, "unit": "columns/s",
+                                  "latency_ms_p50": float(np.percentile(lat, 50)),
+                                  "latency_ms_p99": float(np.percentile(lat, 99)),
+                                  "sample": f"{len(sample)} columns solved one at a time"},
+        "batched_fp64": {"value": batched64_v, "unit": "columns/s"},
+        "speedup_vs_plain_fp64_single_rhs": value / plain_v,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "plane_march_kernel<float,MODE_A>",
+                     "peak_kind": peak_kind},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "wall_s_timed": wall,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

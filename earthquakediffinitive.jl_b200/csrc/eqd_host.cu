@@ -1,0 +1,946 @@
+// libeqd host side: grid set-up, launch geometry, the batched CG driver and
+// the C ABI declared in include/eqd.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/eqd.h"
+#include "ops_tables.h"
+#include "solver_kernels.cuh"
+
+using namespace eqd;
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_OR_RETURN(call)                                                                       \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return fail(e_ == cudaErrorMemoryAllocation ? EQD_ERR_OOM : EQD_ERR_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+        }                                                                                          \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
+        return e;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Launch configuration of the plane-march apply for one precision.
+struct MarchCfg {
+    MarchGeom g;
+    int threads = 0;
+    size_t smem = 0;
+};
+
+static constexpr int kMaxT32 = 640;
+static constexpr int kMaxT64 = 384;
+
+template <typename T>
+static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, int maxt, int tile_rows,
+                           const GridConst &gc, MarchCfg &out, std::string &why) {
+    const int per_row = 2 * n1;
+    int t2 = tile_rows > 0 ? tile_rows : maxt / per_row;
+    t2 = std::min(t2, n2);
+    if (t2 * per_row > maxt) t2 = maxt / per_row;
+    int ntiles = (n2 + t2 - 1) / t2;
+    if (ntiles < 1) ntiles = 1;
+    // Balanced tiles, every tile at least 6 rows (closure reach of the wide operator).
+    while (ntiles > 1 && n2 / ntiles < 6) --ntiles;
+    const int t2max = (n2 + ntiles - 1) / ntiles;
+    if (t2max * per_row > maxt || n2 / ntiles < std::min(6, n2)) {
+        why = "grid too large in x1 for one CTA (n1=" + std::to_string(n1) + ")";
+        return false;
+    }
+    constexpr int AE = 16 / (int)sizeof(T);
+    int CH = (t2max + 2 * EQD_HALO) * n1 + 2 * AE;
+    CH = (CH + AE - 1) / AE * AE;
+    out.g.n1 = n1;
+    out.g.n2 = n2;
+    out.g.n3 = n3;
+    out.g.PS = PS;
+    out.g.colstride = colstride;
+    out.g.ntiles = ntiles;
+    out.g.t2max = t2max;
+    out.g.CH = CH;
+    out.g.i2f0 = gc.i2f0;
+    out.g.n2f = gc.n2f;
+    out.g.i3f0 = gc.i3f0;
+    out.g.n3f = gc.n3f;
+    out.g.nf = gc.nf;
+    int threads = per_row * t2max;
+    threads = (threads + 31) / 32 * 32;
+    out.threads = threads;
+    out.smem = 64 + 32 * 8 + (size_t)EQD_NSLOT * 6 * CH * sizeof(T) + 2 * (size_t)threads * sizeof(T) +
+               2 * (size_t)t2max * 6 * sizeof(T);
+    return true;
+}
+
+template <typename T>
+static void fill_op(OpConst<T> &C, const GridConst &gc, const double h[3]) {
+    for (int a = 0; a < 3; ++a) fill_axis<T>(C.ax[a], a == 0 ? gc.n1 : (a == 1 ? gc.n2 : gc.n3), h[a]);
+    C.lam = (T)gc.lam;
+    C.mu = (T)gc.mu;
+    C.lpm = (T)(gc.lam + gc.mu);
+    C.sat_c = (T)gc.sat_c;
+    C.hvol = gc.hvol;
+}
+
+// Workspace of one batched solve (grown on demand, reused across calls).
+struct Workspace {
+    int cap = 0;            // columns
+    int precision = -1;
+    DevBuf x64, v0, v1, v2, v3;  // x64 + (r, p, q, d) in the working precision
+    DevBuf apply_part, res_part, rr_part;
+    DevBuf gamma, beta, rr_ref, tol, bnorm, iters, status, flag;
+    DevBuf slip_node, slip_comp, slip_dense;
+    DevBuf kout;
+    DevBuf active;
+    int *h_active = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_cap = -1, graph_prec = -1, graph_iters = 0, graph_generic = -1;
+    ~Workspace() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (h_active) cudaFreeHost(h_active);
+    }
+};
+
+struct eqd_grid {
+    eqd_grid_desc desc;
+    GridConst gc;
+    double h[3];
+    OpConst<float> c32;
+    OpConst<double> c64;
+    MarchCfg m32, m64;
+    int nchunks = 1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf err;           // device error word
+    Workspace ws;
+    std::mutex mtx;
+    std::vector<double> x2f, x3f;
+    int tile_rows = 0;
+};
+
+struct eqd_kmat {
+    int device;
+    int n;
+    DevBuf K, s, y, part;
+    cudaStream_t stream = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launch helpers
+// ---------------------------------------------------------------------------
+template <typename T, typename TO, int MODE>
+static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols) {
+    constexpr int MAXT = sizeof(T) == 4 ? kMaxT32 : kMaxT64;
+    const MarchCfg &m = sizeof(T) == 4 ? G->m32 : G->m64;
+    const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
+                                                                               : (const void *)&G->c64);
+    auto kern = plane_march_kernel<T, TO, MODE, MAXT>;
+    cs.ncols = ncols;
+    dim3 grid((unsigned)(ncols * m.g.ntiles));
+    kern<<<grid, m.threads, m.smem, G->stream>>>(C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+    return cudaGetLastError();
+}
+
+// Dynamic shared memory above 48 KB must be opted into per kernel.
+static cudaError_t configure_kernels(int smem_max) {
+    const void *ks[] = {
+        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32>,
+        (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32>,
+        (const void *)plane_march_kernel<float, float, MODE_RHS, kMaxT32>,
+        (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64>,
+        (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64>,
+        (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64>,
+        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64>,
+    };
+    for (const void *k : ks) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+static int check_device_error(eqd_grid *G) {
+    unsigned h = 0;
+    CUDA_OR_RETURN(cudaMemcpyAsync(&h, G->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    if (h != 0) {
+        cudaMemsetAsync(G->err.p, 0, sizeof(unsigned), G->stream);
+        return fail(EQD_ERR_TIMEOUT, "a device-side bounded wait gave up (error word " + std::to_string(h) + ")");
+    }
+    return EQD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Library info
+// ---------------------------------------------------------------------------
+extern "C" const char *eqd_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *eqd_version(void) { return "eqd-b200 0.1 (sm_100a)"; }
+
+extern "C" void eqd_default_opts(eqd_solve_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->rtol = 1e-10;
+    o->atol = 0.0;
+    o->itmax = 0;
+    o->precond = EQD_PRECOND_NONE;
+    o->precision = EQD_PREC_MIXED;
+    o->chunk = 0;
+    o->reliable_delta = 0.1;
+    o->hbm_budget_bytes = 0;
+    o->tile_rows = 0;
+    o->flags = 0;
+}
+
+extern "C" int eqd_device_count(int32_t *count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) n = 0;
+    if (count) *count = n;
+    return n > 0 ? EQD_OK : fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+}
+
+// ---------------------------------------------------------------------------
+// Grid
+// ---------------------------------------------------------------------------
+static bool on_node(double x, double l_f, double tol) { return std::fabs(x) <= l_f + tol; }
+
+extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
+    if (!d || !out) return fail(EQD_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->order != 4) return fail(EQD_ERR_ARG, "only SBP order 4 (standard_diagonal.toml) is supported");
+    if (d->n1 < 9 || d->n2 < 9 || d->n3 < 9)
+        return fail(EQD_ERR_ARG, "SBP order 4 needs at least 9 points per axis (got " + std::to_string(d->n1) + "x" +
+                                     std::to_string(d->n2) + "x" + std::to_string(d->n3) + ")");
+    if (d->n1 > EQD_MAX_N1) return fail(EQD_ERR_ARG, "n1 above the supported maximum of " + std::to_string(EQD_MAX_N1));
+    if (!(d->x1_extent > 0) || !(d->x2_hi > d->x2_lo) || !(d->x3_hi > d->x3_lo))
+        return fail(EQD_ERR_ARG, "empty domain");
+    if (!(d->mu > 0) || !std::isfinite(d->lambda)) return fail(EQD_ERR_ARG, "invalid Lame parameters");
+    if (!(d->l_f >= 0)) return fail(EQD_ERR_ARG, "l_f must be non-negative");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (d->device < 0 || d->device >= ndev) return fail(EQD_ERR_ARG, "device ordinal out of range");
+
+    std::unique_ptr<eqd_grid> G(new eqd_grid());
+    G->desc = *d;
+    GridConst &gc = G->gc;
+    gc.n1 = d->n1;
+    gc.n2 = d->n2;
+    gc.n3 = d->n3;
+    G->h[0] = d->x1_extent / (d->n1 - 1);
+    G->h[1] = (d->x2_hi - d->x2_lo) / (d->n2 - 1);
+    G->h[2] = (d->x3_hi - d->x3_lo) / (d->n3 - 1);
+    gc.PS = (d->n1 * d->n2 + 3) / 4 * 4;
+    gc.colstride = 6LL * d->n3 * gc.PS;
+    gc.lam = d->lambda;
+    gc.mu = d->mu;
+    gc.hvol = G->h[0] * G->h[1] * G->h[2];
+    gc.sat_c = 0.5 / (G->h[0] * kHw[0].v());
+
+    // Omega_f (src/FaultResponse.jl:112-126): |x| <= l_f + 1e-9 max(l_f, 1),
+    // and the extreme selected nodes must sit on -l_f and +l_f.
+    const double tol = 1e-9 * std::max(d->l_f, 1.0);
+    auto select = [&](int n, double lo, double hi, const char *name, int &i0, int &cnt, std::vector<double> &ax) -> int {
+        std::vector<double> x(n);
+        for (int i = 0; i < n; ++i) x[i] = (i == n - 1) ? hi : lo + (hi - lo) * i / (n - 1);
+        i0 = -1;
+        cnt = 0;
+        for (int i = 0; i < n; ++i)
+            if (on_node(x[i], d->l_f, tol)) {
+                if (i0 < 0) i0 = i;
+                ++cnt;
+            }
+        if (cnt == 0) return fail(EQD_ERR_ARG, "no fault nodes inside Omega_f");
+        if (!(std::fabs(x[i0] + d->l_f) <= tol && std::fabs(x[i0 + cnt - 1] - d->l_f) <= tol))
+            return fail(EQD_ERR_ARG, std::string("the elastic grid has no nodes exactly on ") + name +
+                                         " = +-l_f; pick a spacing that divides l_f");
+        ax.assign(x.begin() + i0, x.begin() + i0 + cnt);
+        return EQD_OK;
+    };
+    int rc = select(d->n2, d->x2_lo, d->x2_hi, "x2", gc.i2f0, gc.n2f, G->x2f);
+    if (rc) return rc;
+    rc = select(d->n3, d->x3_lo, d->x3_hi, "x3", gc.i3f0, gc.n3f, G->x3f);
+    if (rc) return rc;
+    gc.nf = gc.n2f * gc.n3f;
+
+    fill_op<float>(G->c32, gc, G->h);
+    fill_op<double>(G->c64, gc, G->h);
+    std::string why;
+    if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT32, 0, gc, G->m32, why) ||
+        !make_march_cfg<double>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT64, 0, gc, G->m64, why))
+        return fail(EQD_ERR_ARG, why);
+    G->nchunks = (int)std::max<long long>(1, (gc.colstride + 16383) / 16384);
+
+    CUDA_OR_RETURN(cudaSetDevice(d->device));
+    {
+        int optin = 0;
+        CUDA_OR_RETURN(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+        if ((size_t)optin < std::max(G->m32.smem, G->m64.smem))
+            return fail(EQD_ERR_ARG, "stencil tile needs more shared memory than the device offers");
+        CUDA_OR_RETURN(configure_kernels((int)std::max(G->m32.smem, G->m64.smem)));
+    }
+    CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
+    CUDA_OR_RETURN(cudaEventCreate(&G->ev0));
+    CUDA_OR_RETURN(cudaEventCreate(&G->ev1));
+    CUDA_OR_RETURN(G->err.ensure(sizeof(unsigned)));
+    CUDA_OR_RETURN(cudaMemset(G->err.p, 0, sizeof(unsigned)));
+    *out = G.release();
+    return EQD_OK;
+}
+
+extern "C" int eqd_grid_destroy(eqd_grid *G) {
+    if (!G) return EQD_OK;
+    cudaSetDevice(G->desc.device);
+    if (G->stream) cudaStreamSynchronize(G->stream);
+    if (G->ev0) cudaEventDestroy(G->ev0);
+    if (G->ev1) cudaEventDestroy(G->ev1);
+    if (G->stream) cudaStreamDestroy(G->stream);
+    delete G;
+    return EQD_OK;
+}
+
+extern "C" int eqd_grid_info(const eqd_grid *G, int64_t *ntot, int32_t *nf, int32_t *n2f, int32_t *n3f) {
+    if (!G) return fail(EQD_ERR_ARG, "null grid");
+    if (ntot) *ntot = 6LL * G->gc.n1 * G->gc.n2 * G->gc.n3;
+    if (nf) *nf = G->gc.nf;
+    if (n2f) *n2f = G->gc.n2f;
+    if (n3f) *n3f = G->gc.n3f;
+    return EQD_OK;
+}
+
+extern "C" int eqd_grid_fault_axes(const eqd_grid *G, double *x2f, double *x3f) {
+    if (!G) return fail(EQD_ERR_ARG, "null grid");
+    if (x2f) std::copy(G->x2f.begin(), G->x2f.end(), x2f);
+    if (x3f) std::copy(G->x3f.begin(), G->x3f.end(), x3f);
+    return EQD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// eqd_apply (operator hook)
+// ---------------------------------------------------------------------------
+template <typename T>
+static int apply_impl(eqd_grid *G, const double *x, double *y, int ncols, int mode) {
+    const GridConst &gc = G->gc;
+    const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
+    DevBuf hx, dx, dy;
+    CUDA_OR_RETURN(hx.ensure(sizeof(double) * ntot * ncols));
+    CUDA_OR_RETURN(dx.ensure(sizeof(T) * gc.colstride * ncols));
+    CUDA_OR_RETURN(dy.ensure(sizeof(T) * gc.colstride * ncols));
+    CUDA_OR_RETURN(cudaMemsetAsync(dx.p, 0, dx.bytes, G->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(hx.p, x, sizeof(double) * ntot * ncols, cudaMemcpyHostToDevice, G->stream));
+    const long long nel = ntot * ncols;
+    const int tb = 256;
+    ref_to_dev_kernel<double, T><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
+        hx.as<double>(), dx.as<T>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, ncols);
+    CUDA_OR_RETURN(cudaGetLastError());
+    ColumnSet cs{};
+    std::vector<int> neg(ncols, -1), zero(ncols, 0);
+    DevBuf sn, sc;
+    CUDA_OR_RETURN(sn.ensure(sizeof(int) * ncols));
+    CUDA_OR_RETURN(sc.ensure(sizeof(int) * ncols));
+    CUDA_OR_RETURN(cudaMemcpyAsync(sn.p, neg.data(), sizeof(int) * ncols, cudaMemcpyHostToDevice, G->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(sc.p, zero.data(), sizeof(int) * ncols, cudaMemcpyHostToDevice, G->stream));
+    cs.slip_node = sn.as<int>();
+    cs.slip_comp = sc.as<int>();
+    if (mode == 0) {
+        CUDA_OR_RETURN((launch_march<T, T, MODE_AP>(G, dx.as<T>(), dy.as<T>(), cs, nullptr, ncols)));
+    } else {
+        CUDA_OR_RETURN((launch_march<T, T, MODE_RHS>(G, dx.as<T>(), dy.as<T>(), cs, nullptr, ncols)));
+    }
+    dev_to_ref_kernel<T, double><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
+        dy.as<T>(), hx.as<double>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, ncols);
+    CUDA_OR_RETURN(cudaGetLastError());
+    CUDA_OR_RETURN(cudaMemcpyAsync(y, hx.p, sizeof(double) * ntot * ncols, cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    return check_device_error(G);
+}
+
+extern "C" int eqd_apply(eqd_grid *G, const double *x, double *y, int32_t ncols, int32_t mode, int32_t precision) {
+    if (!G || !x || !y) return fail(EQD_ERR_ARG, "null argument");
+    if (ncols < 1) return fail(EQD_ERR_ARG, "ncols must be >= 1");
+    if (mode != 0 && mode != 1) return fail(EQD_ERR_ARG, "mode must be 0 (A) or 1 (HP_DSAT)");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    if (precision == EQD_PREC_FP64) return apply_impl<double>(G, x, y, ncols, mode);
+    if (precision == EQD_PREC_MIXED) return apply_impl<float>(G, x, y, ncols, mode);
+    return fail(EQD_ERR_ARG, "unknown precision");
+}
+
+// ---------------------------------------------------------------------------
+// Batched CG driver
+// ---------------------------------------------------------------------------
+struct BatchSpec {
+    int ncols;
+    const int *slip_node;        // host, per column (unit slip), or null
+    const int *slip_comp;
+    const double *slip_dense;    // host [ncols][2][nf] or null
+    const double *rhs;           // host reference-layout RHS [ncols][ntot] (explicit-RHS solve) or null
+    double *u_out;               // host reference-layout solution (explicit-RHS solve) or null
+    double *kcols;               // host 2nf x ncols output (slip-driven) or null
+    double *kdev;                // device 2nf x ncols output (slip-driven) or null
+    int32_t *iters;
+    int8_t *status;
+};
+
+static int resolve_chunk(eqd_grid *G, const eqd_solve_opts &o, int ncols, int prec, int &chunk) {
+    const GridConst &gc = G->gc;
+    const size_t per_col = (size_t)gc.colstride * (prec == EQD_PREC_MIXED ? (8 + 4 * 4) : (8 + 3 * 8)) +
+                           (size_t)16 * gc.nf + 1024;
+    size_t budget = o.hbm_budget_bytes;
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        CUDA_OR_RETURN(cudaMemGetInfo(&fr, &tot));
+        const size_t keep = (size_t)2 << 30;
+        budget = fr > keep ? fr - keep : fr / 2;
+    }
+    long long cap = (long long)(budget / per_col);
+    if (cap < 1) return fail(EQD_ERR_OOM, "HBM budget too small for one column");
+    chunk = o.chunk > 0 ? std::min(o.chunk, ncols) : (int)std::min<long long>(cap, ncols);
+    if ((long long)chunk > cap) chunk = (int)cap;
+    return EQD_OK;
+}
+
+template <typename T>
+static void record_iteration(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, const SolveParams &sp,
+                             const ColState &st) {
+    const int nch = G->nchunks;
+    ColumnSet cs{};
+    cs.ncols = cap;
+    cs.slip_node = W.slip_node.as<int>();
+    cs.slip_comp = W.slip_comp.as<int>();
+    cs.slip_dense = W.slip_dense.p ? W.slip_dense.as<double>() : nullptr;
+    cs.status = W.status.as<int8_t>();
+    T *r = W.v0.as<T>(), *p = W.v1.as<T>(), *q = W.v2.as<T>();
+    if (generic)
+        launch_march<T, T, MODE_AP>(G, p, q, cs, W.apply_part.as<double>(), cap);
+    else
+        launch_march<T, T, MODE_A>(G, p, q, cs, W.apply_part.as<double>(), cap);
+    const unsigned nb = (unsigned)(cap * nch);
+    if (mixed) {
+        cg_update_kernel<float, float><<<nb, 256, 0, G->stream>>>(W.v3.as<float>(), (float *)r, (const float *)p,
+                                                                 (const float *)q, W.apply_part.as<double>(), st, sp,
+                                                                 W.rr_part.as<double>());
+    } else {
+        cg_update_kernel<double, double><<<nb, 256, 0, G->stream>>>(W.x64.as<double>(), (double *)r,
+                                                                   (const double *)p, (const double *)q,
+                                                                   W.apply_part.as<double>(), st, sp,
+                                                                   W.rr_part.as<double>());
+    }
+    const unsigned sb = (unsigned)((cap + 127) / 128);
+    cg_scalar_kernel<<<sb, 128, 0, G->stream>>>(st, sp, W.apply_part.as<double>(), W.rr_part.as<double>(), cap, mixed);
+    if (mixed) {
+        fold_correction_kernel<<<nb, 256, 0, G->stream>>>(W.x64.as<double>(), W.v3.as<float>(), st, sp);
+        ColumnSet cf = cs;
+        cf.flag = W.flag.as<int8_t>();
+        launch_march<double, float, MODE_RHS>(G, W.x64.as<double>(), (float *)r, cf, W.res_part.as<double>(), cap);
+        SolveParams sp2 = sp;
+        sp2.ntiles = G->m64.g.ntiles;
+        cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), cap, 1);
+    }
+    cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(p, r, st, sp);
+}
+
+template <typename T>
+static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, eqd_stats *stats) {
+    const GridConst &gc = G->gc;
+    const int mixed = o.precision == EQD_PREC_MIXED;
+    const int generic = B.rhs != nullptr;
+    const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
+    int chunk = 0;
+    int rc = resolve_chunk(G, o, B.ncols, o.precision, chunk);
+    if (rc) return rc;
+    Workspace &W = G->ws;
+    const size_t vec = (size_t)gc.colstride * chunk;
+    const int nt32 = G->m32.g.ntiles, nt64 = G->m64.g.ntiles;
+    const int ntA = sizeof(T) == 4 ? nt32 : nt64;
+    CUDA_OR_RETURN(W.x64.ensure(sizeof(double) * vec));
+    CUDA_OR_RETURN(W.v0.ensure(sizeof(T) * vec));
+    CUDA_OR_RETURN(W.v1.ensure(sizeof(T) * vec));
+    CUDA_OR_RETURN(W.v2.ensure(sizeof(T) * vec));
+    if (mixed) CUDA_OR_RETURN(W.v3.ensure(sizeof(float) * vec));
+    CUDA_OR_RETURN(W.apply_part.ensure(sizeof(double) * 2 * chunk * std::max(nt32, nt64)));
+    CUDA_OR_RETURN(W.res_part.ensure(sizeof(double) * 2 * chunk * std::max(nt64, G->nchunks)));
+    CUDA_OR_RETURN(W.rr_part.ensure(sizeof(double) * chunk * G->nchunks));
+    for (DevBuf *b : {&W.gamma, &W.beta, &W.rr_ref, &W.tol, &W.bnorm}) CUDA_OR_RETURN(b->ensure(sizeof(double) * chunk));
+    CUDA_OR_RETURN(W.iters.ensure(sizeof(int) * chunk));
+    CUDA_OR_RETURN(W.status.ensure(chunk));
+    CUDA_OR_RETURN(W.flag.ensure(chunk));
+    CUDA_OR_RETURN(W.slip_node.ensure(sizeof(int) * chunk));
+    CUDA_OR_RETURN(W.slip_comp.ensure(sizeof(int) * chunk));
+    if (B.slip_dense) CUDA_OR_RETURN(W.slip_dense.ensure(sizeof(double) * 2 * gc.nf * chunk));
+    else W.slip_dense.release();
+    CUDA_OR_RETURN(W.kout.ensure(sizeof(double) * 2 * gc.nf * chunk));
+    CUDA_OR_RETURN(W.active.ensure(sizeof(int)));
+    if (!W.h_active) CUDA_OR_RETURN(cudaHostAlloc(&W.h_active, sizeof(int), cudaHostAllocDefault));
+    DevBuf hbuf;
+    if (generic) CUDA_OR_RETURN(hbuf.ensure(sizeof(double) * ntot * chunk));
+
+    ColState st{W.gamma.as<double>(), W.beta.as<double>(), W.rr_ref.as<double>(), W.tol.as<double>(),
+                W.bnorm.as<double>(), W.iters.as<int>(), W.status.as<int8_t>(), W.flag.as<int8_t>()};
+    SolveParams sp{};
+    sp.rtol = o.rtol;
+    sp.atol = o.atol;
+    sp.itmax = o.itmax;
+    sp.delta = o.reliable_delta > 0 ? o.reliable_delta : 0.1;
+    sp.ntiles = ntA;
+    sp.nchunks = G->nchunks;
+    sp.colstride = gc.colstride;
+    sp.ntot = ntot;
+
+    // Graph of a few iterations, captured once per (chunk, precision, mode).
+    const int kIter = 10;
+    if (!W.graph || W.graph_cap != chunk || W.graph_prec != o.precision || W.graph_generic != generic) {
+        if (W.graph) cudaGraphExecDestroy(W.graph);
+        W.graph = nullptr;
+        cudaGraph_t g;
+        CUDA_OR_RETURN(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kIter; ++k) record_iteration<T>(G, W, chunk, mixed, generic, sp, st);
+        cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
+        if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&W.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        W.graph_cap = chunk;
+        W.graph_prec = o.precision;
+        W.graph_generic = generic;
+        W.graph_iters = kIter;
+    }
+
+    int64_t tot_it = 0, max_it = 0, unconv = 0, reliable = 0, launches = 0;
+    const int per_iter = mixed ? 7 : 4;
+    float dev_ms_total = 0.f;
+    std::vector<int> hn(chunk), hc(chunk), hit(chunk);
+    std::vector<int8_t> hst(chunk);
+    const int tb = 256;
+    for (int c0 = 0; c0 < B.ncols; c0 += chunk) {
+        const int nc = std::min(chunk, B.ncols - c0);
+        // Column descriptors (unused slots idle).
+        for (int i = 0; i < chunk; ++i) {
+            hn[i] = (i < nc && B.slip_node) ? B.slip_node[c0 + i] : -1;
+            hc[i] = (i < nc && B.slip_comp) ? B.slip_comp[c0 + i] : 0;
+            hst[i] = i < nc ? COL_ACTIVE : COL_IDLE;
+        }
+        CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_node.p, hn.data(), sizeof(int) * chunk, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_comp.p, hc.data(), sizeof(int) * chunk, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(W.status.p, hst.data(), chunk, cudaMemcpyHostToDevice, G->stream));
+        if (B.slip_dense) {
+            CUDA_OR_RETURN(cudaMemsetAsync(W.slip_dense.p, 0, sizeof(double) * 2 * gc.nf * chunk, G->stream));
+            CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_dense.p, B.slip_dense + (size_t)c0 * 2 * gc.nf,
+                                           sizeof(double) * 2 * gc.nf * nc, cudaMemcpyHostToDevice, G->stream));
+        }
+        CUDA_OR_RETURN(cudaMemsetAsync(W.iters.p, 0, sizeof(int) * chunk, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(W.flag.p, 1, chunk, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(W.x64.p, 0, sizeof(double) * vec, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(W.v1.p, 0, sizeof(T) * vec, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(W.v2.p, 0, sizeof(T) * vec, G->stream));
+        if (mixed) CUDA_OR_RETURN(cudaMemsetAsync(W.v3.p, 0, sizeof(float) * vec, G->stream));
+        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+
+        ColumnSet cs{};
+        cs.ncols = chunk;
+        cs.slip_node = W.slip_node.as<int>();
+        cs.slip_comp = W.slip_comp.as<int>();
+        cs.slip_dense = B.slip_dense ? W.slip_dense.as<double>() : nullptr;
+        cs.status = W.status.as<int8_t>();
+        const unsigned sb = (unsigned)((chunk + 127) / 128);
+        if (!generic) {
+            // r0 = b = H P (D+SAT) chi  (x = 0), in the working precision.
+            CUDA_OR_RETURN((launch_march<double, T, MODE_RHS>(G, W.x64.as<double>(), W.v0.as<T>(), cs,
+                                                               W.res_part.as<double>(), chunk)));
+            SolveParams sp2 = sp;
+            sp2.ntiles = nt64;
+            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), chunk, mixed);
+        } else {
+            // r0 = b given explicitly (reference layout, FP64).
+            CUDA_OR_RETURN(cudaMemsetAsync(W.v0.p, 0, sizeof(T) * vec, G->stream));
+            CUDA_OR_RETURN(cudaMemcpyAsync(hbuf.p, B.rhs + (size_t)c0 * ntot, sizeof(double) * ntot * nc,
+                                           cudaMemcpyHostToDevice, G->stream));
+            const long long nel = ntot * nc;
+            ref_to_dev_kernel<double, T><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
+                hbuf.as<double>(), W.v0.as<T>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, nc);
+            // ||b||^2 through the update kernel's reduction with alpha = 0.
+            CUDA_OR_RETURN(cudaMemsetAsync(W.apply_part.p, 0, sizeof(double) * 2 * chunk * ntA, G->stream));
+            cg_update_kernel<T, double><<<(unsigned)(chunk * G->nchunks), 256, 0, G->stream>>>(
+                W.x64.as<double>(), W.v0.as<T>(), W.v1.as<T>(), W.v2.as<T>(), W.apply_part.as<double>(), st, sp,
+                W.rr_part.as<double>());
+            SolveParams sp2 = sp;
+            sp2.ntiles = G->nchunks;
+            // rr_part has stride 1; copy into the stride-2 layout the kernel reads.
+            CUDA_OR_RETURN(cudaMemsetAsync(W.res_part.p, 0, sizeof(double) * 2 * chunk * G->nchunks, G->stream));
+            CUDA_OR_RETURN(cudaMemcpy2DAsync(W.res_part.p, 2 * sizeof(double), W.rr_part.p, sizeof(double),
+                                             sizeof(double), (size_t)chunk * G->nchunks, cudaMemcpyDeviceToDevice,
+                                             G->stream));
+            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), chunk, 0);
+        }
+        cg_pupdate_kernel<T><<<(unsigned)(chunk * G->nchunks), 256, 0, G->stream>>>(W.v1.as<T>(), W.v0.as<T>(), st, sp);
+        CUDA_OR_RETURN(cudaGetLastError());
+        launches += generic ? 4 : 3;
+
+        const long long itmax = o.itmax > 0 ? o.itmax : 2 * ntot;
+        long long launched = 0;
+        for (;;) {
+            count_active_kernel<<<1, 256, 0, G->stream>>>(W.status.as<int8_t>(), chunk, W.active.as<int>());
+            CUDA_OR_RETURN(cudaMemcpyAsync(W.h_active, W.active.p, sizeof(int), cudaMemcpyDeviceToHost, G->stream));
+            CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+            if (*W.h_active == 0) break;
+            if (launched > itmax + kIter) break;
+            CUDA_OR_RETURN(cudaGraphLaunch(W.graph, G->stream));
+            launched += kIter;
+            launches += 1 + (int64_t)kIter * per_iter;
+        }
+        launches += 1;
+        rc = check_device_error(G);
+        if (rc) return rc;
+
+        // Outputs.
+        if (!generic) {
+            ExtractGeom eg{gc.n1, gc.n2, gc.n3, gc.PS, gc.nf, gc.i2f0, gc.n2f, gc.i3f0, gc.n3f, gc.colstride, gc.mu};
+            const long long nthr = (long long)nc * gc.nf;
+            ColumnSet ce = cs;
+            ce.ncols = nc;
+            double *kdst = B.kdev ? B.kdev + (size_t)c0 * 2 * gc.nf : W.kout.as<double>();
+            extract_traction_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, G->stream>>>(
+                G->c64, eg, W.x64.as<double>(), ce, kdst, 2LL * gc.nf);
+            CUDA_OR_RETURN(cudaGetLastError());
+            launches += 1;
+        }
+        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+        if (!generic && B.kcols) {
+            CUDA_OR_RETURN(cudaMemcpyAsync(B.kcols + (size_t)c0 * 2 * gc.nf, W.kout.p, sizeof(double) * 2 * gc.nf * nc,
+                                           cudaMemcpyDeviceToHost, G->stream));
+        }
+        if (generic && B.u_out) {
+            const long long nel = ntot * nc;
+            dev_to_ref_kernel<double, double><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
+                W.x64.as<double>(), hbuf.as<double>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, nc);
+            CUDA_OR_RETURN(cudaMemcpyAsync(B.u_out + (size_t)c0 * ntot, hbuf.p, sizeof(double) * ntot * nc,
+                                           cudaMemcpyDeviceToHost, G->stream));
+        }
+        CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), W.iters.p, sizeof(int) * chunk, cudaMemcpyDeviceToHost, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), W.status.p, chunk, cudaMemcpyDeviceToHost, G->stream));
+        CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, G->ev0, G->ev1);
+        dev_ms_total += ms;
+        for (int i = 0; i < nc; ++i) {
+            tot_it += hit[i];
+            max_it = std::max<int64_t>(max_it, hit[i]);
+            if (hst[i] != COL_CONVERGED) ++unconv;
+            if (B.iters) B.iters[c0 + i] = hit[i];
+            if (B.status) B.status[c0 + i] = hst[i] == COL_ACTIVE ? (int8_t)EQD_COL_MAXITER : hst[i];
+        }
+    }
+    if (stats) {
+        stats->solves += B.ncols;
+        stats->iterations += tot_it;
+        stats->max_iterations = std::max<int64_t>(stats->max_iterations, max_it);
+        stats->unconverged += unconv;
+        stats->reliable_updates += reliable;
+        stats->kernel_launches += launches;
+        stats->device_seconds += dev_ms_total * 1e-3;
+        stats->precision = o.precision;
+        stats->precond = o.precond;
+    }
+    if ((o.flags & EQD_FLAG_STRICT) && unconv > 0)
+        return fail(EQD_ERR_NOT_CONVERGED, std::to_string(unconv) + " column(s) did not converge");
+    return EQD_OK;
+}
+
+static int run_batch_any(eqd_grid *G, const eqd_solve_opts *opts, const BatchSpec &B, eqd_stats *stats) {
+    eqd_solve_opts o;
+    if (opts) o = *opts;
+    else eqd_default_opts(&o);
+    if (!(o.rtol >= 0) || !(o.atol >= 0)) return fail(EQD_ERR_ARG, "rtol/atol must be non-negative");
+    if (o.precond == EQD_PRECOND_JACOBI)
+        return fail(EQD_ERR_UNSUPPORTED, "precond=:jacobi is not available on this path");
+    if (o.precond != EQD_PRECOND_NONE) return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
+    if (o.precision != EQD_PREC_FP64 && o.precision != EQD_PREC_MIXED) return fail(EQD_ERR_ARG, "unknown precision");
+    if (B.rhs && o.precision != EQD_PREC_FP64) return fail(EQD_ERR_UNSUPPORTED, "explicit-RHS solves run in FP64");
+    const auto t0 = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(G->mtx);
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    int rc = o.precision == EQD_PREC_MIXED ? run_batch<float>(G, o, B, stats) : run_batch<double>(G, o, B, stats);
+    if (stats)
+        stats->seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+extern "C" int eqd_stiffness_columns(eqd_grid *G, const int32_t *cols, int32_t ncols, const eqd_solve_opts *opts,
+                                     double *out, int32_t *iters, int8_t *status, eqd_stats *stats) {
+    if (!G || (!cols && ncols > 0) || (!out && ncols > 0)) return fail(EQD_ERR_ARG, "null argument");
+    if (ncols < 0) return fail(EQD_ERR_ARG, "ncols must be >= 0");
+    if (ncols == 0) return EQD_OK;
+    const int nf = G->gc.nf;
+    std::vector<int> node(ncols), comp(ncols);
+    for (int i = 0; i < ncols; ++i) {
+        if (cols[i] < 0 || cols[i] >= 2 * nf) return fail(EQD_ERR_ARG, "column index out of range");
+        node[i] = cols[i] < nf ? cols[i] : cols[i] - nf;
+        comp[i] = cols[i] < nf ? 0 : 1;
+    }
+    BatchSpec B{};
+    B.ncols = ncols;
+    B.slip_node = node.data();
+    B.slip_comp = comp.data();
+    B.kcols = out;
+    B.iters = iters;
+    B.status = status;
+    return run_batch_any(G, opts, B, stats);
+}
+
+extern "C" int eqd_stiffness_columns_device(eqd_grid *G, const int32_t *cols, int32_t ncols,
+                                            const eqd_solve_opts *opts, double *out_device, int32_t *iters,
+                                            int8_t *status, eqd_stats *stats) {
+    if (!G || (!cols && ncols > 0) || (!out_device && ncols > 0)) return fail(EQD_ERR_ARG, "null argument");
+    if (ncols < 0) return fail(EQD_ERR_ARG, "ncols must be >= 0");
+    if (ncols == 0) return EQD_OK;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, out_device) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
+        pa.device != G->desc.device) {
+        cudaGetLastError();
+        return fail(EQD_ERR_ARG, "out_device is not device memory of the grid's device");
+    }
+    const int nf = G->gc.nf;
+    std::vector<int> node(ncols), comp(ncols);
+    for (int i = 0; i < ncols; ++i) {
+        if (cols[i] < 0 || cols[i] >= 2 * nf) return fail(EQD_ERR_ARG, "column index out of range");
+        node[i] = cols[i] < nf ? cols[i] : cols[i] - nf;
+        comp[i] = cols[i] < nf ? 0 : 1;
+    }
+    BatchSpec B{};
+    B.ncols = ncols;
+    B.slip_node = node.data();
+    B.slip_comp = comp.data();
+    B.kdev = out_device;
+    B.iters = iters;
+    B.status = status;
+    return run_batch_any(G, opts, B, stats);
+}
+
+extern "C" int eqd_stiffness_exact(eqd_grid *G, const eqd_solve_opts *opts, double *K, eqd_stats *stats) {
+    if (!G || !K) return fail(EQD_ERR_ARG, "null argument");
+    const int n = 2 * G->gc.nf;
+    std::vector<int32_t> cols(n);
+    for (int i = 0; i < n; ++i) cols[i] = i;
+    return eqd_stiffness_columns(G, cols.data(), n, opts, K, nullptr, nullptr, stats);
+}
+
+extern "C" int eqd_shear_traction(eqd_grid *G, const double *s2, const double *s3, int32_t nslip, double *dtau2,
+                                  double *dtau3, const eqd_solve_opts *opts, eqd_stats *stats) {
+    if (!G || !s2 || !s3 || !dtau2 || !dtau3) return fail(EQD_ERR_ARG, "null argument");
+    if (nslip < 1) return fail(EQD_ERR_ARG, "nslip must be >= 1");
+    const int nf = G->gc.nf;
+    std::vector<double> dense((size_t)nslip * 2 * nf);
+    for (int c = 0; c < nslip; ++c)
+        for (int k = 0; k < nf; ++k) {
+            dense[((size_t)c * 2 + 0) * nf + k] = s2[(size_t)c * nf + k];
+            dense[((size_t)c * 2 + 1) * nf + k] = s3[(size_t)c * nf + k];
+        }
+    std::vector<int> node(nslip, -1), comp(nslip, 0);
+    std::vector<double> out((size_t)2 * nf * nslip);
+    BatchSpec B{};
+    B.ncols = nslip;
+    B.slip_node = node.data();
+    B.slip_comp = comp.data();
+    B.slip_dense = dense.data();
+    B.kcols = out.data();
+    int rc = run_batch_any(G, opts, B, stats);
+    if (rc) return rc;
+    for (int c = 0; c < nslip; ++c)
+        for (int k = 0; k < nf; ++k) {
+            dtau2[(size_t)c * nf + k] = out[(size_t)c * 2 * nf + k];
+            dtau3[(size_t)c * nf + k] = out[(size_t)c * 2 * nf + nf + k];
+        }
+    return EQD_OK;
+}
+
+extern "C" int eqd_cg_solve(eqd_grid *G, const double *rhs, double *u, int32_t ncols, const eqd_solve_opts *opts,
+                            int32_t *iters, int8_t *status, eqd_stats *stats) {
+    if (!G || !rhs || !u) return fail(EQD_ERR_ARG, "null argument");
+    if (ncols < 1) return fail(EQD_ERR_ARG, "ncols must be >= 1");
+    eqd_solve_opts o;
+    if (opts) o = *opts;
+    else eqd_default_opts(&o);
+    o.precision = EQD_PREC_FP64;
+    BatchSpec B{};
+    B.ncols = ncols;
+    B.rhs = rhs;
+    B.u_out = u;
+    B.iters = iters;
+    B.status = status;
+    return run_batch_any(G, &o, B, stats);
+}
+
+extern "C" int eqd_stiffness_toeplitz(eqd_grid *G, const eqd_solve_opts *opts, double *K, eqd_stats *stats) {
+    if (!G || !K) return fail(EQD_ERR_ARG, "null argument");
+    const GridConst &gc = G->gc;
+    const int n2 = gc.n2f, n3 = gc.n3f, nf = gc.nf;
+    // Sources in priority order: centre, then the corners (1-based (a, b)).
+    const int ac = (n2 + 1) / 2, bc = (n3 + 1) / 2;
+    const int sa[5] = {ac, 1, n2, 1, n2}, sb[5] = {bc, 1, 1, n3, n3};
+    std::vector<int32_t> cols(10);
+    for (int s = 0; s < 5; ++s) {
+        const int node = (sb[s] - 1) * n2 + (sa[s] - 1);
+        cols[2 * s] = node;
+        cols[2 * s + 1] = nf + node;
+    }
+    std::vector<double> resp((size_t)10 * 2 * nf);
+    int rc = eqd_stiffness_columns(G, cols.data(), 10, opts, resp.data(), nullptr, nullptr, stats);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(G->mtx);
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    const size_t N = 2 * (size_t)nf;
+    DevBuf dK, dsrc, da, db;
+    CUDA_OR_RETURN(dK.ensure(sizeof(double) * N * N));
+    CUDA_OR_RETURN(dsrc.ensure(sizeof(double) * resp.size()));
+    CUDA_OR_RETURN(da.ensure(sizeof(int) * 5));
+    CUDA_OR_RETURN(db.ensure(sizeof(int) * 5));
+    CUDA_OR_RETURN(cudaMemcpyAsync(dsrc.p, resp.data(), sizeof(double) * resp.size(), cudaMemcpyHostToDevice, G->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(da.p, sa, sizeof(sa), cudaMemcpyHostToDevice, G->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(db.p, sb, sizeof(sb), cudaMemcpyHostToDevice, G->stream));
+    const long long ne = (long long)nf * nf;
+    toeplitz_expand_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, G->stream>>>(dsrc.as<double>(), da.as<int>(),
+                                                                              db.as<int>(), 5, n2, n3, dK.as<double>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    CUDA_OR_RETURN(cudaMemcpyAsync(K, dK.p, sizeof(double) * N * N, cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    return EQD_OK;
+}
+
+template <typename T>
+static int profile_apply_impl(eqd_grid *G, int ncols, int warmup, int reps, double *ms, double *bytes) {
+    const GridConst &gc = G->gc;
+    DevBuf x, y, part;
+    const long long n = gc.colstride * (long long)ncols;
+    CUDA_OR_RETURN(x.ensure(sizeof(T) * n));
+    CUDA_OR_RETURN(y.ensure(sizeof(T) * n));
+    const int nt = sizeof(T) == 4 ? G->m32.g.ntiles : G->m64.g.ntiles;
+    CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * nt));
+    fill_random_kernel<T><<<1184, 256, 0, G->stream>>>(x.as<T>(), n, 12345ull);
+    CUDA_OR_RETURN(cudaGetLastError());
+    ColumnSet cs{};
+    for (int i = 0; i < warmup; ++i)
+        CUDA_OR_RETURN((launch_march<T, T, MODE_A>(G, x.as<T>(), y.as<T>(), cs, part.as<double>(), ncols)));
+    CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+    for (int i = 0; i < reps; ++i)
+        CUDA_OR_RETURN((launch_march<T, T, MODE_A>(G, x.as<T>(), y.as<T>(), cs, part.as<double>(), ncols)));
+    CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+    CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
+    float t = 0.f;
+    CUDA_OR_RETURN(cudaEventElapsedTime(&t, G->ev0, G->ev1));
+    if (ms) *ms = (double)t / std::max(reps, 1);
+    if (bytes) *bytes = 2.0 * 6.0 * gc.n1 * gc.n2 * gc.n3 * sizeof(T) * ncols;
+    return check_device_error(G);
+}
+
+extern "C" int eqd_profile_apply(eqd_grid *G, int32_t ncols, int32_t precision, int32_t warmup, int32_t reps,
+                                 double *ms_per_launch, double *bytes_per_launch) {
+    if (!G || ncols < 1 || reps < 1 || warmup < 0) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    if (precision == EQD_PREC_MIXED) return profile_apply_impl<float>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
+    if (precision == EQD_PREC_FP64) return profile_apply_impl<double>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
+    return fail(EQD_ERR_ARG, "unknown precision");
+}
+
+extern "C" int eqd_diag(eqd_grid *G, double *d) {
+    (void)G;
+    (void)d;
+    return fail(EQD_ERR_UNSUPPORTED, "eqd_diag is not implemented yet");
+}
+
+// ---------------------------------------------------------------------------
+// Resident K and the time-loop GEMV
+// ---------------------------------------------------------------------------
+extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out) {
+    if (!out || !K || n < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev) return fail(EQD_ERR_ARG, "device ordinal out of range");
+    CUDA_OR_RETURN(cudaSetDevice(device));
+    std::unique_ptr<eqd_kmat> M(new eqd_kmat());
+    M->device = device;
+    M->n = n;
+    CUDA_OR_RETURN(M->K.ensure(sizeof(double) * (size_t)n * n));
+    CUDA_OR_RETURN(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
+    CUDA_OR_RETURN(cudaMemcpyAsync(M->K.p, K, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, M->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
+    *out = M.release();
+    return EQD_OK;
+}
+
+static int gemv_slices(int n) {
+    // Enough CTAs to cover every SM several times over.
+    const int rows_blocks = (n / 2 + 255) / 256;
+    int s = std::max(1, (148 * 8) / std::max(1, rows_blocks));
+    return std::min(s, std::max(1, n / 64));
+}
+
+extern "C" int eqd_kmat_gemv(eqd_kmat *M, const double *s, double *y, int32_t nvec) {
+    if (!M || !s || !y || nvec < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    CUDA_OR_RETURN(cudaSetDevice(M->device));
+    const int n = M->n;
+    const int nslice = gemv_slices(n);
+    CUDA_OR_RETURN(M->s.ensure(sizeof(double) * (size_t)n * nvec));
+    CUDA_OR_RETURN(M->y.ensure(sizeof(double) * (size_t)n * nvec));
+    CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)n * nvec * nslice));
+    CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, sizeof(double) * (size_t)n * nvec, cudaMemcpyHostToDevice, M->stream));
+    dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
+    gemv_partial_kernel<<<grid, 256, 0, M->stream>>>(M->K.as<double>(), M->s.as<double>(), n, nslice, nvec,
+                                                     M->part.as<double>());
+    const long long ne = (long long)n * nvec;
+    gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, M->stream>>>(M->part.as<double>(), n, nslice, nvec,
+                                                                           M->y.as<double>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, sizeof(double) * (size_t)n * nvec, cudaMemcpyDeviceToHost, M->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
+    return EQD_OK;
+}
+
+extern "C" int eqd_kmat_destroy(eqd_kmat *M) {
+    if (!M) return EQD_OK;
+    cudaSetDevice(M->device);
+    if (M->stream) {
+        cudaStreamSynchronize(M->stream);
+        cudaStreamDestroy(M->stream);
+    }
+    delete M;
+    return EQD_OK;
+}

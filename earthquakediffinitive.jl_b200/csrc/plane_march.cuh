@@ -1,0 +1,535 @@
+// Matrix-free split-node SBP-SAT elastic operator, one sweep per column.
+//
+// Computes, for every column of a batch, one of
+//   MODE_A   : y = -H P (D + SAT) v          (v already in range(P))
+//   MODE_AP  : y = -H P (D + SAT) P x        (generic x; P applied in smem)
+//   MODE_RHS : y = +H P (D + SAT) (x + chi)  (x in range(P); chi from the
+//              column's slip) = b - A x, the true residual of the CG system
+// where, per side, D is the constant-coefficient Navier operator
+//   (D v)_j = mu * sum_a D2_a v_j + mu * D2_j v_j + lam * D1_j D1_j v_j
+//             + (lam + mu) * sum_{k != j} D1_j D1_k v_k
+// (`elastic_blocks`, src/Elasticity.jl:80-89), SAT adds
+// c * (tau_j^+ - tau_j^-) with c = 1 / (2 h1 w_0) on both fault faces
+// (src/ElasticitySplitNode.jl:149-162 with `_prolongation`, :63-68), and P
+// zeroes far-field rows and averages the two sides of each fault node
+// (:171-203). The traction tau is `traction_blocks` (src/Elasticity.jl:195-221).
+//
+// Factorisation used here (exact in real arithmetic, reference composes the
+// same D1 matrices):
+//   w_1 = mu (2 D2_1 + D2_2 + D2_3) v_1 + D1_1 F_1
+//   w_2 = mu (D2_1 + 2 D2_2 + D2_3) v_2 + lam W_2 v_2
+//         + (lam + mu) (D1_1 H21 + D1_3 H23)
+//   w_3 = mu (D2_1 + D2_2 + 2 D2_3) v_3 + D1_3 F_3
+// with G_k = D1_k v_k, F_1 = lam G_1 + (lam+mu)(G_2+G_3),
+// F_3 = lam G_3 + (lam+mu)(G_1+G_2), H21 = D1_2 v_1, H23 = D1_2 v_3 and
+// W_2 = D1_2 D1_2 (the wide operator, as a 1D matrix).
+//
+// Work decomposition (one CTA per (column, x2-tile)):
+//   * threads = both sides x all n1 points x the tile's x2 rows;
+//   * x1 derivatives read the thread's own line from shared memory;
+//   * x2 derivatives read neighbouring rows (tile + 4-row halo) from shared;
+//   * x3 is marched plane by plane; x3 derivatives come from 7-deep register
+//     windows (closure rows reach +-3 planes);
+//   * planes arrive through a 6-slot ring filled by cp.async.bulk copies
+//     completing on mbarriers, three planes ahead of use.
+#pragma once
+#include "eqd_common.cuh"
+
+namespace eqd {
+
+enum { MODE_A = 0, MODE_AP = 1, MODE_RHS = 2 };
+
+// Per-axis operator tables, built on the host from the exact 1D matrices of
+// that axis length (so overlapping closures of short axes are exact).
+//   *_cl[r][o]    : full rows of the 4 closure rows at each end, offsets -3..3
+//                   (r = 0..3 lower end rows 0..3; r = 4..7 upper end rows
+//                   n-1..n-4)
+//   *_corrL[r][k] : row r minus the interior stencil, columns k (lower end)
+//   *_corrR[r][k] : row n-1-r minus the interior stencil, columns n-1-k
+template <typename T>
+struct AxisT {
+    T d1_int[5], d2_int[5], w_int[9];
+    T d1_corrL[4][6], d1_corrR[4][6];
+    T d2_corrL[4][6], d2_corrR[4][6];
+    T w_corrL[6][10], w_corrR[6][10];
+    T d1_cl[8][7], d2_cl[8][7];
+    T dlo[4];
+    T wq[4];
+};
+
+template <typename T>
+struct OpConst {
+    AxisT<T> ax[3];
+    T lam, mu, lpm;        // lam + mu
+    T sat_c;
+    double hvol;
+};
+
+struct MarchGeom {
+    int n1, n2, n3, PS;
+    long long colstride;
+    int ntiles;            // x2 tiles per column
+    int t2max;             // rows per tile (upper bound)
+    int CH;                // ring chunk capacity (elements) per (side, comp)
+    int i2f0, n2f, i3f0, n3f, nf;
+};
+
+// Out-of-range window entries are zero and meet zero coefficients.
+template <typename T>
+__device__ __forceinline__ T x3_d1(const OpConst<T> &C, const T (&w)[7], int q, int n3) {
+    const AxisT<T> &a = C.ax[2];
+    if (q >= 4 && q <= n3 - 5)
+        return a.d1_int[0] * w[1] + a.d1_int[1] * w[2] + a.d1_int[3] * w[4] + a.d1_int[4] * w[5];
+    const int r = q < 4 ? q : 4 + (n3 - 1 - q);
+    T s = T(0);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) s += a.d1_cl[r][o] * w[o];
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T x3_d2(const OpConst<T> &C, const T (&w)[7], int q, int n3) {
+    const AxisT<T> &a = C.ax[2];
+    if (q >= 4 && q <= n3 - 5)
+        return a.d2_int[0] * w[1] + a.d2_int[1] * w[2] + a.d2_int[2] * w[3] + a.d2_int[3] * w[4] +
+               a.d2_int[4] * w[5];
+    const int r = q < 4 ? q : 4 + (n3 - 1 - q);
+    T s = T(0);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) s += a.d2_cl[r][o] * w[o];
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void shift7(T (&w)[7], T v) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = w[k + 1];
+    w[6] = v;
+}
+
+// x2-direction D1 / D2 / W at row r of a chunk pointer `c` (own element),
+// row stride n1. Interior stencil everywhere (rows beyond the domain read
+// zeros), plus the closure correction on the first/last rows.
+template <typename T>
+__device__ __forceinline__ T x2_d1(const AxisT<T> &a, const T *c, int n1, int r, int n2) {
+    T s = a.d1_int[0] * c[-2 * n1] + a.d1_int[1] * c[-n1] + a.d1_int[3] * c[n1] + a.d1_int[4] * c[2 * n1];
+    if (r < 4) {
+        const T *b = c - r * n1;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s += a.d1_corrL[r][k] * b[k * n1];
+    } else if (r >= n2 - 4) {
+        const int rr = n2 - 1 - r;
+        const T *b = c + rr * n1;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s += a.d1_corrR[rr][k] * b[-k * n1];
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T x2_d2(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2) {
+    T s = a.d2_int[0] * c[-2 * n1] + a.d2_int[1] * c[-n1] + a.d2_int[2] * self + a.d2_int[3] * c[n1] +
+          a.d2_int[4] * c[2 * n1];
+    if (r < 4) {
+        const T *b = c - r * n1;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s += a.d2_corrL[r][k] * b[k * n1];
+    } else if (r >= n2 - 4) {
+        const int rr = n2 - 1 - r;
+        const T *b = c + rr * n1;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s += a.d2_corrR[rr][k] * b[-k * n1];
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T x2_w(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2) {
+    T s = a.w_int[4] * self;
+#pragma unroll
+    for (int o = 1; o <= 4; ++o) s += a.w_int[4 - o] * c[-o * n1] + a.w_int[4 + o] * c[o * n1];
+    if (r < 6) {
+        const T *b = c - r * n1;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) s += a.w_corrL[r][k] * b[k * n1];
+    } else if (r >= n2 - 6) {
+        const int rr = n2 - 1 - r;
+        const T *b = c + rr * n1;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) s += a.w_corrR[rr][k] * b[-k * n1];
+    }
+    return s;
+}
+
+template <typename T, typename TO, int MODE, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__ MarchGeom g,
+                   const T *__restrict__ in, TO *__restrict__ out, ColumnSet cs,
+                   double *__restrict__ partials, unsigned *__restrict__ err) {
+    const int col = blockIdx.x / g.ntiles;
+    const int tile = blockIdx.x % g.ntiles;
+    if (col >= cs.ncols) return;
+    if (cs.status && cs.status[col] != COL_ACTIVE) return;
+    if (cs.flag && !cs.flag[col]) return;
+
+    const int n1 = g.n1, n2 = g.n2, n3 = g.n3;
+    const int a0 = (int)((long long)tile * n2 / g.ntiles);
+    const int a1 = (int)((long long)(tile + 1) * n2 / g.ntiles);
+    constexpr int AE = 16 / (int)sizeof(T);  // elements per 16 bytes
+
+    // Row range copied per plane (tile + halo, clipped), 16-byte aligned.
+    const int r0 = max(a0 - EQD_HALO, 0), r1 = min(a1 + EQD_HALO, n2);
+    const int lo_el = (a0 - EQD_HALO) * n1;
+    const int base = lo_el >= 0 ? (lo_el / AE) * AE : -(((-lo_el) + AE - 1) / AE) * AE;
+    const int e0 = ((r0 * n1) / AE) * AE;
+    const int e1 = ((r1 * n1 + AE - 1) / AE) * AE;
+    const unsigned bytes = (unsigned)((e1 - e0) * (int)sizeof(T));
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw);
+    double *red = reinterpret_cast<double *>(smem_raw + 64);
+    T *ring = reinterpret_cast<T *>(smem_raw + 64 + 32 * 8);
+    const int NT = blockDim.x;
+    T *xF1 = ring + (size_t)EQD_NSLOT * 6 * g.CH;
+    T *xH21 = xF1 + NT;
+    T *face = xH21 + NT;  // [2][t2max][6]
+
+    const int tid = threadIdx.x;
+    const int per_side = n1 * g.t2max;
+    const int side = tid / per_side;
+    const int rem = tid - side * per_side;
+    const int i2l = rem / n1;
+    const int i1 = rem - i2l * n1;
+    const int i2 = a0 + i2l;
+    const bool valid = (side < 2) && (i2 < a1);
+
+    const T *incol = in + (long long)col * g.colstride;
+    TO *outcol = out + (long long)col * g.colstride;
+
+    // Zero the ring (rows outside the domain must read as zero), init barriers.
+    {
+        const int nring = EQD_NSLOT * 6 * g.CH;
+        for (int i = tid; i < nring; i += NT) ring[i] = T(0);
+        fence_proxy_async_smem();
+        if (tid == 0) {
+            for (int k = 0; k < EQD_NSLOT; ++k) mbar_init(&mbar[k], 1);
+            fence_mbar_init();
+        }
+    }
+    __syncthreads();
+
+    auto issue_plane = [&](int q) {
+        const int slot = q % EQD_NSLOT;
+        mbar_arrive_expect_tx(&mbar[slot], 6u * bytes);
+        for (int sc = 0; sc < 6; ++sc) {
+            T *dst = ring + ((size_t)slot * 6 + sc) * g.CH + (e0 - base);
+            const T *src = incol + ((long long)sc * n3 + q) * g.PS + e0;
+            bulk_g2s(dst, src, bytes, &mbar[slot]);
+        }
+    };
+    int issued = min(EQD_NSLOT, n3), dead_at = 0;
+    if (tid == 0) {
+        for (int q = 0; q < issued; ++q) issue_plane(q);
+    }
+
+    // Per-thread x1 row operators (start column within the line + 6 taps).
+    const AxisT<T> &A1 = C.ax[0];
+    int s1;
+    T c1[6], c2[6];
+    if (i1 < 4) {
+        s1 = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int o = k - i1;  // offset from the row
+            c1[k] = (o >= -3 && o <= 3) ? A1.d1_cl[i1][o + 3] : T(0);
+            c2[k] = (o >= -3 && o <= 3) ? A1.d2_cl[i1][o + 3] : T(0);
+        }
+    } else if (i1 >= n1 - 4) {
+        s1 = n1 - 6;
+        const int rr = n1 - 1 - i1;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int o = (s1 + k) - i1;
+            c1[k] = (o >= -3 && o <= 3) ? A1.d1_cl[4 + rr][o + 3] : T(0);
+            c2[k] = (o >= -3 && o <= 3) ? A1.d2_cl[4 + rr][o + 3] : T(0);
+        }
+    } else {
+        s1 = i1 - 2;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) { c1[k] = A1.d1_int[k]; c2[k] = A1.d2_int[k]; }
+        c1[5] = T(0);
+        c2[5] = T(0);
+    }
+    const bool is_face = valid && ((side == 0 && i1 == n1 - 1) || (side == 1 && i1 == 0));
+    const bool ff_x12 = (side == 0 && i1 == 0) || (side == 1 && i1 == n1 - 1) || i2 == 0 || i2 == n2 - 1;
+    const T wq1 = (i1 < 4) ? A1.wq[i1] : (i1 >= n1 - 4 ? A1.wq[n1 - 1 - i1] : T(1));
+    const T wq2 = (i2 < 4) ? C.ax[1].wq[i2] : (i2 >= n2 - 4 ? C.ax[1].wq[n2 - 1 - i2] : T(1));
+    const double hpt = C.hvol * (double)wq1 * (double)wq2 * (MODE == MODE_RHS ? 1.0 : -1.0);
+
+    const int own = i2 * n1 + i1 - base;                   // offset inside a chunk
+    const int lineoff = i2 * n1 + s1 - base;               // x1 window start
+    const int fidx = (side * g.t2max + i2l) * 6;           // my face record
+    const int oidx = ((1 - side) * g.t2max + i2l) * 6;     // partner's face record
+    const long long ooff = (long long)i2 * n1 + i1;        // plane offset in global
+
+    T v1w[7], v2w[7], v3w[7], F3w[7], H23w[7], w3q[3];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) { v1w[k] = v2w[k] = v3w[k] = F3w[k] = H23w[k] = T(0); }
+    w3q[0] = w3q[1] = w3q[2] = T(0);
+
+    double acc0 = 0.0, acc1 = 0.0;
+    bool dead = false;
+
+    const T lam = C.lam, mu = C.mu, lpm = C.lpm;
+    const AxisT<T> &A2 = C.ax[1];
+
+    for (int s = 0; s < n3 + 6; ++s) {
+        // ---- ingest plane s -------------------------------------------------
+        if (s < n3) {
+            const int slot = s % EQD_NSLOT;
+            if (!mbar_wait_bounded(&mbar[slot], (unsigned)((s / EQD_NSLOT) & 1), err)) dead = true;
+            if (MODE != MODE_A) {
+                // Fix-up pass on the landed plane: chi (RHS) or P (generic input).
+                T *pl = ring + (size_t)slot * 6 * g.CH;
+                const int nrows = r1 - r0;
+                if (MODE == MODE_RHS) {
+                    if (s >= g.i3f0 && s < g.i3f0 + g.n3f) {
+                        for (int w = tid; w < nrows; w += NT) {
+                            const int r = r0 + w;
+                            if (r < g.i2f0 || r >= g.i2f0 + g.n2f) continue;
+                            const int k = (r - g.i2f0) + g.n2f * (s - g.i3f0);
+                            for (int j = 0; j < 2; ++j) {
+                                double sl;
+                                if (cs.slip_dense)
+                                    sl = cs.slip_dense[((long long)col * 2 + j) * g.nf + k];
+                                else
+                                    sl = (cs.slip_node[col] == k && cs.slip_comp[col] == j) ? 1.0 : 0.0;
+                                if (sl != 0.0) {
+                                    pl[(0 * 3 + 1 + j) * g.CH + r * n1 + (n1 - 1) - base] -= (T)(0.5 * sl);
+                                    pl[(1 * 3 + 1 + j) * g.CH + r * n1 + 0 - base] += (T)(0.5 * sl);
+                                }
+                            }
+                        }
+                    }
+                } else {  // MODE_AP: v = P x
+                    const bool plane_ff = (s == 0 || s == n3 - 1);
+                    for (int w = tid; w < nrows * 3; w += NT) {
+                        const int r = r0 + w / 3, j = w % 3;
+                        T *m = pl + (0 * 3 + j) * g.CH + r * n1 - base;
+                        T *p = pl + (1 * 3 + j) * g.CH + r * n1 - base;
+                        if (plane_ff || r == 0 || r == n2 - 1) {
+                            for (int i = 0; i < n1; ++i) { m[i] = T(0); p[i] = T(0); }
+                        } else {
+                            m[0] = T(0);
+                            p[n1 - 1] = T(0);
+                            const T avg = T(0.5) * (m[n1 - 1] + p[0]);
+                            m[n1 - 1] = avg;
+                            p[0] = avg;
+                        }
+                    }
+                }
+                fence_proxy_async_smem();
+                __syncthreads();
+            }
+            if (__syncthreads_or(dead)) {
+                dead = true;
+                dead_at = s;
+                break;
+            }
+            const T *pl = ring + (size_t)slot * 6 * g.CH;
+            const T *c3 = pl + (side * 3 + 2) * g.CH + own;
+            T a = T(0), b = T(0), c = T(0), h = T(0);
+            if (valid) {
+                a = pl[(side * 3 + 0) * g.CH + own];
+                b = pl[(side * 3 + 1) * g.CH + own];
+                c = c3[0];
+                h = x2_d1(A2, c3, n1, i2, n2);
+            }
+            shift7(v1w, a);
+            shift7(v2w, b);
+            shift7(v3w, c);
+            shift7(H23w, h);
+        } else {
+            shift7(v1w, T(0));
+            shift7(v2w, T(0));
+            shift7(v3w, T(0));
+            shift7(H23w, T(0));
+        }
+
+        // ---- in-plane work at p = s - 3 ---------------------------------------
+        const int p = s - 3;
+        T w1 = T(0), w2 = T(0), w3p = T(0), F3 = T(0);
+        T tau1 = T(0), tau2 = T(0), tau3 = T(0);
+        if (p >= 0 && p < n3 && valid) {
+            const T *pl = ring + (size_t)(p % EQD_NSLOT) * 6 * g.CH;
+            const T *l1 = pl + (side * 3 + 0) * g.CH + lineoff;
+            const T *l2 = pl + (side * 3 + 1) * g.CH + lineoff;
+            const T *l3 = pl + (side * 3 + 2) * g.CH + lineoff;
+            const T *o1 = pl + (side * 3 + 0) * g.CH + own;
+            const T *o2 = pl + (side * 3 + 1) * g.CH + own;
+            const T *o3 = pl + (side * 3 + 2) * g.CH + own;
+            const T v1 = v1w[3], v2 = v2w[3], v3 = v3w[3];
+            // x1 direction: G1 and D2_1 of each component, boundary derivatives.
+            T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const T x1 = l1[k], x2 = l2[k], x3 = l3[k];
+                G1 += c1[k] * x1;
+                A11 += c2[k] * x1;
+                A21 += c2[k] * x2;
+                A31 += c2[k] * x3;
+            }
+            // x2 direction.
+            const T G2 = x2_d1(A2, o2, n1, i2, n2);
+            const T H21 = x2_d1(A2, o1, n1, i2, n2);
+            const T A12 = x2_d2(A2, o1, v1, n1, i2, n2);
+            const T A22 = x2_d2(A2, o2, v2, n1, i2, n2);
+            const T A32 = x2_d2(A2, o3, v3, n1, i2, n2);
+            const T W2 = x2_w(A2, o2, v2, n1, i2, n2);
+            // x3 direction (register windows centred on p).
+            const T G3 = x3_d1(C, v3w, p, n3);
+            const T A13 = x3_d2(C, v1w, p, n3);
+            const T A23 = x3_d2(C, v2w, p, n3);
+            const T A33 = x3_d2(C, v3w, p, n3);
+            const T D3H23 = x3_d1(C, H23w, p, n3);
+
+            const T F1 = lam * G1 + lpm * (G2 + G3);
+            F3 = lam * G3 + lpm * (G1 + G2);
+            xF1[tid] = F1;
+            xH21[tid] = H21;
+            w1 = mu * (T(2) * A11 + A12 + A13);
+            w2 = mu * (A21 + T(2) * A22 + A23) + lam * W2 + lpm * D3H23;
+            w3p = mu * (A31 + A32 + T(2) * A33);
+            if (is_face) {
+                // +x1 boundary derivative at the fault node: lower end of the
+                // plus block (window cols 0..3), upper end of the minus block
+                // (window cols 5..2, odd mirror).
+                T dh1 = T(0), dh2 = T(0), dh3 = T(0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int q = side == 1 ? k : 5 - k;
+                    const T cf = side == 1 ? A1.dlo[k] : -A1.dlo[k];
+                    dh1 += cf * l1[q];
+                    dh2 += cf * l2[q];
+                    dh3 += cf * l3[q];
+                }
+                const T D3v1 = x3_d1(C, v1w, p, n3);
+                tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
+                tau2 = mu * (H21 + dh2);
+                tau3 = mu * (D3v1 + dh3);
+                face[fidx + 0] = tau1;
+                face[fidx + 1] = tau2;
+                face[fidx + 2] = tau3;
+            }
+        }
+        __syncthreads();
+        if (p >= 0 && p < n3 && valid) {
+            const int lb = tid - i1 + s1;  // x1 window start in the exchange arrays
+            T E1 = T(0), E21 = T(0);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                E1 += c1[k] * xF1[lb + k];
+                E21 += c1[k] * xH21[lb + k];
+            }
+            w1 += E1;
+            w2 += lpm * E21;
+            if (is_face) {
+                // SAT: c (tau^+ - tau^-), added on both faces.
+                const T sgn = side == 0 ? T(-1) : T(1);
+                w1 += C.sat_c * sgn * (tau1 - face[oidx + 0]);
+                w2 += C.sat_c * sgn * (tau2 - face[oidx + 1]);
+                w3p += C.sat_c * sgn * (tau3 - face[oidx + 2]);
+            }
+        }
+        // Queue w3's partial (needs D1_3 F3 three planes later), window F3.
+        const T w3z_part = w3q[0];
+        w3q[0] = w3q[1];
+        w3q[1] = w3q[2];
+        w3q[2] = w3p;
+        shift7(F3w, F3);
+        const int z = s - 6;
+        T w3 = T(0);
+        if (z >= 0 && z < n3 && valid) w3 = w3z_part + x3_d1(C, F3w, z, n3);
+        if (is_face) {
+            face[fidx + 3] = w1;
+            face[fidx + 4] = w2;
+            face[fidx + 5] = w3;
+        }
+        __syncthreads();
+
+        // ---- epilogue: P, H, store, dot partials ------------------------------
+        if (valid) {
+            if (p >= 0 && p < n3) {
+                const bool ff = ff_x12 || p == 0 || p == n3 - 1;
+                const int rq = p < 4 ? p : (p >= n3 - 4 ? n3 - 1 - p : -1);
+                const double hw = hpt * (rq >= 0 ? (double)C.ax[2].wq[rq] : 1.0);
+                double y1 = 0.0, y2 = 0.0;
+                if (!ff) {
+                    T u1 = w1, u2 = w2;
+                    if (is_face) {
+                        u1 = T(0.5) * (w1 + face[oidx + 3]);
+                        u2 = T(0.5) * (w2 + face[oidx + 4]);
+                    }
+                    y1 = hw * (double)u1;
+                    y2 = hw * (double)u2;
+                }
+                const long long o = ((long long)(side * 3 + 0) * n3 + p) * g.PS + ooff;
+                outcol[o] = (TO)y1;
+                outcol[o + (long long)n3 * g.PS] = (TO)y2;
+                if (MODE == MODE_RHS) {
+                    acc0 += (double)(TO)y1 * (double)(TO)y1 + (double)(TO)y2 * (double)(TO)y2;
+                } else {
+                    acc0 += (double)v1w[3] * (double)(TO)y1 + (double)v2w[3] * (double)(TO)y2;
+                    acc1 += (double)v1w[3] * (double)v1w[3] + (double)v2w[3] * (double)v2w[3];
+                }
+            }
+            if (z >= 0 && z < n3) {
+                const bool ff = ff_x12 || z == 0 || z == n3 - 1;
+                const int rq = z < 4 ? z : (z >= n3 - 4 ? n3 - 1 - z : -1);
+                const double hw = hpt * (rq >= 0 ? (double)C.ax[2].wq[rq] : 1.0);
+                double y3 = 0.0;
+                if (!ff) {
+                    T u3 = w3;
+                    if (is_face) u3 = T(0.5) * (w3 + face[oidx + 5]);
+                    y3 = hw * (double)u3;
+                }
+                const long long o = ((long long)(side * 3 + 2) * n3 + z) * g.PS + ooff;
+                outcol[o] = (TO)y3;
+                if (MODE == MODE_RHS) {
+                    acc0 += (double)(TO)y3 * (double)(TO)y3;
+                } else {
+                    acc0 += (double)v3w[0] * (double)(TO)y3;
+                    acc1 += (double)v3w[0] * (double)v3w[0];
+                }
+            }
+        }
+        // Slot of plane p is free once every thread passed the barrier above.
+        if (s >= 3 && s + 3 < n3) {
+            if (tid == 0) issue_plane(s + 3);
+            issued = s + 4;
+        }
+    }
+
+    if (dead) {
+        // A wait gave up (recorded in *err). Before the CTA's shared memory is
+        // released, wait (bounded) for every plane copy issued and not yet
+        // consumed: planes dead_at .. issued-1.
+        if (tid == 0) {
+            for (int q = dead_at; q < issued; ++q)
+                mbar_wait_bounded(&mbar[q % EQD_NSLOT], (unsigned)((q / EQD_NSLOT) & 1), err);
+        }
+        __syncthreads();
+        return;
+    }
+
+    const double s0 = block_sum(acc0, red);
+    __syncthreads();
+    const double s1v = block_sum(acc1, red);
+    if (tid == 0 && partials) {
+        double *pp = partials + ((long long)col * g.ntiles + tile) * 2;
+        pp[0] = s0;
+        pp[1] = s1v;
+    }
+}
+
+}  // namespace eqd

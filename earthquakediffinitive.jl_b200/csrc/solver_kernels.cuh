@@ -1,0 +1,418 @@
+// Batched conjugate-gradient vector kernels, per-column scalar logic,
+// traction extraction, Toeplitz expansion, dense GEMV and layout transforms.
+//
+// Every reduction is per column and in a fixed order (block tree, then the
+// partials of that column in index order), so a column's result does not
+// depend on which other columns share its batch.
+#pragma once
+#include "plane_march.cuh"
+
+namespace eqd {
+
+// Per-column CG state (device).
+struct ColState {
+    double *gamma;      // r.r of the current search direction
+    double *beta;
+    double *rr_ref;     // true ||r||^2 at the last reliable update (mixed)
+    double *tol;        // atol + rtol ||b||
+    double *bnorm;
+    int *iters;
+    int8_t *status;
+    int8_t *flag;       // mixed: reliable update pending this iteration
+};
+
+struct SolveParams {
+    double rtol, atol;
+    long long itmax;    // 0 -> 2 * Ntot (the Krylov default)
+    double delta;       // mixed: reliable update when ||r|| < delta * ||r_ref||
+    int ntiles;         // apply partials per column
+    int nchunks;        // update partials per column
+    long long colstride;
+    long long ntot;     // unpadded DOF count (for itmax default)
+};
+
+// ---------------------------------------------------------------------------
+// x += alpha p ; r -= alpha q ; partial r.r   (alpha = gamma / p.q)
+// X is the solution accumulator (FP64 for plain CG, FP32 correction d for the
+// mixed inner solve).
+// ---------------------------------------------------------------------------
+template <typename T, typename TX>
+__global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *__restrict__ r,
+                                                        const T *__restrict__ p, const T *__restrict__ q,
+                                                        const double *__restrict__ apply_part, ColState st,
+                                                        SolveParams sp, double *__restrict__ rr_part) {
+    const int col = blockIdx.x / sp.nchunks;
+    const int chunk = blockIdx.x % sp.nchunks;
+    if (st.status[col] != COL_ACTIVE) return;
+    __shared__ double red[32];
+    __shared__ double s_alpha;
+    if (threadIdx.x == 0) {
+        double pq = 0.0, pp = 0.0;
+        for (int t = 0; t < sp.ntiles; ++t) {
+            pq += apply_part[((long long)col * sp.ntiles + t) * 2 + 0];
+            pp += apply_part[((long long)col * sp.ntiles + t) * 2 + 1];
+        }
+        double a = st.gamma[col] / pq;
+        if (!(pq > 2.220446049250313e-16 * pp) || !isfinite(a)) a = 0.0;  // breakdown: scalar kernel flags it
+        s_alpha = a;
+    }
+    __syncthreads();
+    const double alpha = s_alpha;
+    const long long n = sp.colstride;
+    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+    const long long off = (long long)col * n;
+    double acc = 0.0;
+    const T a_t = (T)alpha;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        const T pi = p[off + i], qi = q[off + i];
+        x[off + i] = (TX)(x[off + i] + (TX)alpha * (TX)pi);
+        const T ri = r[off + i] - a_t * qi;
+        r[off + i] = ri;
+        acc += (double)ri * (double)ri;
+    }
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) rr_part[(long long)col * sp.nchunks + chunk] = s;
+}
+
+// p = r + beta p for active columns.
+template <typename T>
+__global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, const T *__restrict__ r, ColState st,
+                                                         SolveParams sp) {
+    const int col = blockIdx.x / sp.nchunks;
+    const int chunk = blockIdx.x % sp.nchunks;
+    if (st.status[col] != COL_ACTIVE) return;
+    const T b = (T)st.beta[col];
+    const long long n = sp.colstride;
+    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+    const long long off = (long long)col * n;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) p[off + i] = r[off + i] + b * p[off + i];
+}
+
+// Mixed precision: fold the FP32 correction into the FP64 solution.
+__global__ void __launch_bounds__(256) fold_correction_kernel(double *__restrict__ x, float *__restrict__ d, ColState st,
+                                                              SolveParams sp) {
+    const int col = blockIdx.x / sp.nchunks;
+    const int chunk = blockIdx.x % sp.nchunks;
+    if (st.status[col] != COL_ACTIVE || !st.flag[col]) return;
+    const long long n = sp.colstride;
+    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+    const long long off = (long long)col * n;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        x[off + i] += (double)d[off + i];
+        d[off + i] = 0.f;
+    }
+}
+
+__device__ __forceinline__ double sum_parts(const double *part, int col, int n, int stride, int k) {
+    double s = 0.0;
+    for (int t = 0; t < n; ++t) s += part[((long long)col * n + t) * stride + k];
+    return s;
+}
+
+// After the update: count the iteration, test convergence (plain: Krylov's
+// rule on the recursive residual), choose beta, or flag a reliable update.
+__global__ void cg_scalar_kernel(ColState st, SolveParams sp, const double *__restrict__ apply_part,
+                                 const double *__restrict__ rr_part, int ncols, int mixed) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncols || st.status[col] != COL_ACTIVE) return;
+    const double pq = sum_parts(apply_part, col, sp.ntiles, 2, 0);
+    const double pp = sum_parts(apply_part, col, sp.ntiles, 2, 1);
+    const double rr = sum_parts(rr_part, col, sp.nchunks, 1, 0);
+    const long long itmax = sp.itmax > 0 ? sp.itmax : 2 * sp.ntot;
+    const int it = st.iters[col] + 1;
+    st.iters[col] = it;
+    if (!(pq > 2.220446049250313e-16 * pp)) {  // zero / negative curvature
+        if (mixed) {
+            st.flag[col] = 1;  // let the true residual decide
+            return;
+        }
+        st.status[col] = COL_BREAKDOWN;
+        return;
+    }
+    if (!isfinite(rr)) {
+        st.status[col] = COL_NONFINITE;
+        return;
+    }
+    if (!mixed) {
+        if (sqrt(rr) <= st.tol[col]) {
+            st.status[col] = COL_CONVERGED;
+        } else if (it >= itmax) {
+            st.status[col] = COL_MAXITER;
+        } else {
+            st.beta[col] = rr / st.gamma[col];
+            st.gamma[col] = rr;
+        }
+        return;
+    }
+    const double tol = st.tol[col];
+    if (rr <= tol * tol || rr <= sp.delta * sp.delta * st.rr_ref[col] || it >= itmax) {
+        st.flag[col] = 1;
+    } else {
+        st.beta[col] = rr / st.gamma[col];
+        st.gamma[col] = rr;
+        st.flag[col] = 0;
+    }
+}
+
+// After a true-residual evaluation (start of a solve, or a reliable update).
+// `first`: this is r0 = b (sets ||b|| and the tolerance).
+__global__ void cg_true_residual_kernel(ColState st, SolveParams sp, const double *__restrict__ res_part, int ncols,
+                                        int mixed) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncols || st.status[col] != COL_ACTIVE) return;
+    if (mixed && !st.flag[col]) return;
+    const double rr = sum_parts(res_part, col, sp.ntiles, 2, 0);
+    const int it = st.iters[col];
+    if (it == 0) {
+        const double bn = sqrt(rr);
+        st.bnorm[col] = bn;
+        st.tol[col] = sp.atol + sp.rtol * bn;
+        st.beta[col] = 0.0;
+        st.gamma[col] = rr;
+        st.rr_ref[col] = rr;
+        st.flag[col] = 0;
+        if (rr == 0.0) st.status[col] = COL_CONVERGED;  // x = 0 solves it exactly
+        else if (!isfinite(rr)) st.status[col] = COL_NONFINITE;
+        else if (bn <= st.tol[col]) st.status[col] = COL_CONVERGED;
+        return;
+    }
+    const long long itmax = sp.itmax > 0 ? sp.itmax : 2 * sp.ntot;
+    st.flag[col] = 0;
+    if (!isfinite(rr)) {
+        st.status[col] = COL_NONFINITE;
+    } else if (sqrt(rr) <= st.tol[col]) {
+        st.status[col] = COL_CONVERGED;
+    } else if (it >= itmax) {
+        st.status[col] = COL_MAXITER;
+    } else {
+        st.beta[col] = rr / st.gamma[col];
+        st.gamma[col] = rr;
+        st.rr_ref[col] = rr;
+    }
+}
+
+__global__ void count_active_kernel(const int8_t *__restrict__ status, int ncols, int *__restrict__ out) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int c = 0;
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) c += status[i] == COL_ACTIVE;
+    atomicAdd(&cnt, c);
+    __syncthreads();
+    if (threadIdx.x == 0) *out = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// Traction extraction: K column entries from U = x + chi (FP64).
+//   dtau_j(k) = 1/2 (tau_j^-(U^-) + tau_j^+(U^+)),  j = 2, 3,
+//   tau_j = mu (D1_j U_1 + dhat U_j) at the fault node
+// (`shear_traction!`, src/FaultResponse.jl:201-211, with T2/T3 of :130-132).
+// One thread per (column, Omega_f node).
+// ---------------------------------------------------------------------------
+struct ExtractGeom {
+    int n1, n2, n3, PS, nf, i2f0, n2f, i3f0, n3f;
+    long long colstride;
+    double mu;
+};
+
+// Full D1 row r of an axis of length n applied to f(0..n-1).
+template <typename F>
+__device__ __forceinline__ double d1_row(const AxisT<double> &a, int n, int r, F f) {
+    double s = 0.0;
+    for (int o = -2; o <= 2; ++o) {
+        const int c = r + o;
+        if (o != 0 && c >= 0 && c < n) s += a.d1_int[o + 2] * f(c);
+    }
+    if (r < 4) {
+        for (int k = 0; k < 6; ++k) s += a.d1_corrL[r][k] * f(k);
+    } else if (r >= n - 4) {
+        const int rr = n - 1 - r;
+        for (int k = 0; k < 6; ++k) s += a.d1_corrR[rr][k] * f(n - 1 - k);
+    }
+    return s;
+}
+
+__global__ void extract_traction_kernel(const __grid_constant__ OpConst<double> C, ExtractGeom g,
+                                        const double *__restrict__ x, ColumnSet cs, double *__restrict__ K,
+                                        long long kld) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = (int)(gid / g.nf);
+    const int k = (int)(gid % g.nf);
+    if (col >= cs.ncols) return;
+    const int a = k % g.n2f, b = k / g.n2f;
+    const int i2 = g.i2f0 + a, i3 = g.i3f0 + b;
+    const int n1 = g.n1, n2 = g.n2, n3 = g.n3;
+    const double *xc = x + (long long)col * g.colstride;
+    auto chi = [&](int side, int comp, int ii2, int ii3) -> double {
+        // chi of this column at the fault node (ii2, ii3), component comp (1, 2).
+        if (comp == 0) return 0.0;
+        if (ii2 < g.i2f0 || ii2 >= g.i2f0 + g.n2f || ii3 < g.i3f0 || ii3 >= g.i3f0 + g.n3f) return 0.0;
+        const int kk = (ii2 - g.i2f0) + g.n2f * (ii3 - g.i3f0);
+        double sl;
+        if (cs.slip_dense)
+            sl = cs.slip_dense[((long long)col * 2 + (comp - 1)) * g.nf + kk];
+        else
+            sl = (cs.slip_node[col] == kk && cs.slip_comp[col] == comp - 1) ? 1.0 : 0.0;
+        return side == 0 ? -0.5 * sl : 0.5 * sl;
+    };
+    auto U = [&](int side, int comp, int ii1, int ii2, int ii3) -> double {
+        double v = xc[((long long)(side * 3 + comp) * n3 + ii3) * g.PS + (long long)ii2 * n1 + ii1];
+        const int fi1 = side == 0 ? n1 - 1 : 0;
+        if (ii1 == fi1) v += chi(side, comp, ii2, ii3);
+        return v;
+    };
+    double dt[2];
+    for (int j = 0; j < 2; ++j) {  // j = 0 -> tau_2 (x2), j = 1 -> tau_3 (x3)
+        double t = 0.0;
+        for (int side = 0; side < 2; ++side) {
+            const int fi1 = side == 0 ? n1 - 1 : 0;
+            // tangential derivative of U_1 along x2 (j=0) or x3 (j=1)
+            double tang;
+            if (j == 0)
+                tang = d1_row(C.ax[1], n2, i2, [&](int c) { return U(side, 0, fi1, c, i3); });
+            else
+                tang = d1_row(C.ax[2], n3, i3, [&](int c) { return U(side, 0, fi1, i2, c); });
+            // boundary derivative of U_{j+1} along +x1
+            double dh = 0.0;
+            for (int q = 0; q < 4; ++q) {
+                if (side == 1) dh += C.ax[0].dlo[q] * U(side, j + 1, q, i2, i3);
+                else dh -= C.ax[0].dlo[q] * U(side, j + 1, n1 - 1 - q, i2, i3);
+            }
+            t += g.mu * (tang + dh);
+        }
+        dt[j] = 0.5 * t;
+    }
+    K[(long long)col * kld + k] = dt[0];
+    K[(long long)col * kld + g.nf + k] = dt[1];
+}
+
+// ---------------------------------------------------------------------------
+// Toeplitz expansion (`fault_stiffness_toeplitz`, src/FaultResponse.jl:339-393):
+// K[i, j] from the response of the first source (priority order) that
+// reaches the separation (a_i - a_j, b_i - b_j); unreachable -> 0.
+// src_cols: [5 sources][2 (s2, s3)][2nf] responses, src_a/src_b 1-based.
+// ---------------------------------------------------------------------------
+__global__ void toeplitz_expand_kernel(const double *__restrict__ src_cols, const int *__restrict__ src_a,
+                                       const int *__restrict__ src_b, int nsrc, int n2f, int n3f,
+                                       double *__restrict__ K) {
+    const int nf = n2f * n3f;
+    const long long N = 2LL * nf;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nf * nf) return;
+    const int i = (int)(gid % nf), j = (int)(gid / nf);
+    const int ai = i % n2f + 1, bi = i / n2f + 1, aj = j % n2f + 1, bj = j / n2f + 1;
+    const int da = ai - aj, db = bi - bj;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    for (int s = 0; s < nsrc; ++s) {
+        const int a = src_a[s] + da, b = src_b[s] + db;
+        if (a >= 1 && a <= n2f && b >= 1 && b <= n3f) {
+            const int node = (b - 1) * n2f + (a - 1);
+            const double *c2 = src_cols + (long long)(s * 2 + 0) * N;
+            const double *c3 = src_cols + (long long)(s * 2 + 1) * N;
+            v0 = c2[node];
+            v1 = c2[nf + node];
+            v2 = c3[node];
+            v3 = c3[nf + node];
+            break;
+        }
+    }
+    K[(long long)j * N + i] = v0;
+    K[(long long)j * N + nf + i] = v1;
+    K[(long long)(nf + j) * N + i] = v2;
+    K[(long long)(nf + j) * N + nf + i] = v3;
+}
+
+// ---------------------------------------------------------------------------
+// Dense FP64 GEMV y = K s (K column-major n x n), two passes: column slices
+// write partial row sums, then a fixed-order reduction over slices.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restrict__ K, const double *__restrict__ s,
+                                                           long long n, int nslice, int nvec,
+                                                           double *__restrict__ part) {
+    const long long row2 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+    const int slice = blockIdx.y;
+    const long long c0 = n * slice / nslice, c1 = n * (slice + 1) / nslice;
+    for (int v = 0; v < nvec; ++v) {
+        const double *sv = s + (long long)v * n;
+        double a0 = 0.0, a1 = 0.0;
+        if (row2 + 1 < n) {
+            long long c = c0;
+            for (; c + 4 <= c1; c += 4) {
+                const double2 k0 = *reinterpret_cast<const double2 *>(K + c * n + row2);
+                const double2 k1 = *reinterpret_cast<const double2 *>(K + (c + 1) * n + row2);
+                const double2 k2 = *reinterpret_cast<const double2 *>(K + (c + 2) * n + row2);
+                const double2 k3 = *reinterpret_cast<const double2 *>(K + (c + 3) * n + row2);
+                const double s0 = sv[c], s1 = sv[c + 1], s2 = sv[c + 2], s3 = sv[c + 3];
+                a0 += k0.x * s0 + k1.x * s1 + k2.x * s2 + k3.x * s3;
+                a1 += k0.y * s0 + k1.y * s1 + k2.y * s2 + k3.y * s3;
+            }
+            for (; c < c1; ++c) {
+                const double2 kk = *reinterpret_cast<const double2 *>(K + c * n + row2);
+                a0 += kk.x * sv[c];
+                a1 += kk.y * sv[c];
+            }
+            part[((long long)v * nslice + slice) * n + row2] = a0;
+            part[((long long)v * nslice + slice) * n + row2 + 1] = a1;
+        } else if (row2 < n) {
+            for (long long c = c0; c < c1; ++c) a0 += K[c * n + row2] * sv[c];
+            part[((long long)v * nslice + slice) * n + row2] = a0;
+        }
+    }
+}
+
+__global__ void gemv_reduce_kernel(const double *__restrict__ part, long long n, int nslice, int nvec,
+                                   double *__restrict__ y) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n * nvec) return;
+    const int v = (int)(gid / n);
+    const long long row = gid % n;
+    double s = 0.0;
+    for (int t = 0; t < nslice; ++t) s += part[((long long)v * nslice + t) * n + row];
+    y[gid] = s;
+}
+
+// Deterministic pseudo-random fill in [-1, 1) (measurement inputs).
+template <typename T>
+__global__ void fill_random_kernel(T *__restrict__ v, long long n, unsigned long long seed) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = (unsigned long long)i + seed * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        v[i] = (T)((double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Layout transforms: reference DOF order (per column, Ntot contiguous) <->
+// padded device layout. `T`/`U` allow precision conversion.
+// ---------------------------------------------------------------------------
+template <typename TS, typename TD>
+__global__ void ref_to_dev_kernel(const TS *__restrict__ src, TD *__restrict__ dst, int n1, int n2, int n3, int PS,
+                                  long long colstride, int ncols) {
+    const long long N = (long long)n1 * n2 * n3;
+    const long long ntot = 6 * N;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= ntot * ncols) return;
+    const int col = (int)(gid / ntot);
+    const long long r = gid % ntot;
+    const long long sc = r / N, pt = r % N;
+    const long long i3 = pt / ((long long)n1 * n2), pl = pt % ((long long)n1 * n2);
+    dst[(long long)col * colstride + (sc * n3 + i3) * PS + pl] = (TD)src[gid];
+}
+
+template <typename TS, typename TD>
+__global__ void dev_to_ref_kernel(const TS *__restrict__ src, TD *__restrict__ dst, int n1, int n2, int n3, int PS,
+                                  long long colstride, int ncols) {
+    const long long N = (long long)n1 * n2 * n3;
+    const long long ntot = 6 * N;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= ntot * ncols) return;
+    const int col = (int)(gid / ntot);
+    const long long r = gid % ntot;
+    const long long sc = r / N, pt = r % N;
+    const long long i3 = pt / ((long long)n1 * n2), pl = pt % ((long long)n1 * n2);
+    dst[gid] = (TD)src[(long long)col * colstride + (sc * n3 + i3) * PS + pl];
+}
+
+}  // namespace eqd

@@ -1,0 +1,189 @@
+/*
+ * libeqd — B200 (sm_100a) fault-stiffness engine, C ABI.
+ *
+ * Drop-in for the dense fault-stiffness path of EarthquakeDiffinitive.jl:
+ * one CG solve per unit-slip right-hand side on the split-node SBP-SAT
+ * elastic operator A = -H P (D + SAT) P, assembled into K : [s2; s3] -> [dtau2; dtau3].
+ * The Julia side binds these with `ccall`. All buffers in
+ * the signatures are HOST memory owned by the caller; the library owns its
+ * device memory. Matrices are column-major FP64, exactly the layout of the
+ * reference's `Matrix{Float64}`.
+ *
+ * Conventions shared with the reference:
+ *   - Omega_f nodes are ordered x2-fastest over an (n2f, n3f) grid
+ *     (src/FaultResponse.jl:112-126).
+ *   - K column c < nf is the response to unit s2 at node c, column nf + c to
+ *     unit s3 at node c; rows 0..nf-1 are dtau2, nf..2nf-1 dtau3
+ *     (src/FaultResponse.jl:249-255).
+ *   - A "reference-layout" vector has Ntot = 6 n1 n2 n3 entries ordered
+ *     [u1- u2- u3- u1+ u2+ u3+], each block x1-fastest
+ *     (src/ElasticitySplitNode.jl:36-42).
+ *
+ * Every call returns an eqd_status; eqd_last_error() describes the last
+ * failure on the calling thread.
+ */
+#ifndef EQD_H
+#define EQD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    EQD_OK = 0,
+    EQD_ERR_ARG = 1,          /* invalid argument (the reference's error() cases) */
+    EQD_ERR_OOM = 2,          /* device allocation failed / over the HBM budget   */
+    EQD_ERR_CUDA = 3,         /* CUDA runtime error                               */
+    EQD_ERR_NOT_CONVERGED = 4,/* returned only when opts.flags has EQD_FLAG_STRICT */
+    EQD_ERR_TIMEOUT = 5,      /* a device-side bounded wait gave up               */
+    EQD_ERR_UNSUPPORTED = 6,
+    EQD_ERR_NO_DEVICE = 7
+} eqd_status;
+
+/* Per-column solve outcome. */
+typedef enum {
+    EQD_COL_CONVERGED = 1,
+    EQD_COL_MAXITER = 2,
+    EQD_COL_BREAKDOWN = 3,    /* p.Ap <= eps |p|^2 (Krylov's zero curvature) */
+    EQD_COL_NONFINITE = 4
+} eqd_col_status;
+
+typedef enum {
+    EQD_PREC_FP64 = 0,        /* plain FP64 CG, Krylov.jl cg! rule (recursive residual) */
+    EQD_PREC_MIXED = 1        /* FP32 CG with FP64 reliable updates; stops on the FP64 true residual */
+} eqd_precision;
+
+typedef enum { EQD_PRECOND_NONE = 0, EQD_PRECOND_JACOBI = 1 } eqd_precond;
+
+#define EQD_FLAG_STRICT 1u    /* return EQD_ERR_NOT_CONVERGED if any column did not converge */
+
+/*
+ * Two equidistant blocks meeting at the fault plane x1 = 0:
+ *   minus block x1 in [-x1_extent, 0], plus block x1 in [0, x1_extent],
+ *   both x2 in [x2_lo, x2_hi], x3 in [x3_lo, x3_hi], n1 x n2 x n3 nodes each.
+ * Replaces the grid pair built in `build_model` (src/BP8.jl:196-206) and the
+ * `FaultElasticity(g_minus, g_plus, λ, μ, set; l_f)` constructor
+ * (src/FaultResponse.jl:96-146): Omega_f = nodes with |x2|, |x3| <= l_f, which
+ * must land exactly on grid nodes (same tolerance and error as the reference).
+ */
+typedef struct {
+    int32_t n1, n2, n3;
+    double x1_extent;
+    double x2_lo, x2_hi, x3_lo, x3_hi;
+    double lambda, mu;
+    double l_f;
+    int32_t order;            /* must be 4 (standard_diagonal.toml, order 4) */
+    int32_t device;           /* CUDA device ordinal */
+} eqd_grid_desc;
+
+/* Mirrors `CGSolver(A; rtol=1e-10, atol=0.0, itmax=0, precond=:none)`
+ * (src/ElasticitySplitNode.jl:365) plus the B200 engine's knobs. */
+typedef struct {
+    double rtol;              /* default 1e-10 */
+    double atol;              /* default 0 */
+    int64_t itmax;            /* 0 -> 2 Ntot, Krylov's default */
+    int32_t precond;          /* eqd_precond */
+    int32_t precision;        /* eqd_precision */
+    int32_t chunk;            /* columns per device batch; 0 -> as many as the HBM budget allows */
+    double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.1) */
+    uint64_t hbm_budget_bytes;/* 0 -> free device memory minus 2 GiB */
+    int32_t tile_rows;        /* x2 rows per CTA tile in the stencil; 0 -> autotuned */
+    uint32_t flags;
+} eqd_solve_opts;
+
+/* Mirrors `CGStats` + `solver_report` (src/ElasticitySplitNode.jl:256-262, 442-447). */
+typedef struct {
+    int64_t solves;
+    int64_t iterations;
+    int64_t max_iterations;
+    int64_t unconverged;
+    int64_t reliable_updates; /* mixed precision only */
+    double seconds;           /* wall time of the call */
+    double device_seconds;    /* CUDA-event time of the solve loop */
+    int32_t precond;
+    int32_t precision;
+    int64_t kernel_launches;  /* libeqd kernels launched by the call (graph nodes included) */
+} eqd_stats;
+
+typedef struct eqd_grid eqd_grid;
+typedef struct eqd_kmat eqd_kmat;
+typedef struct eqd_server eqd_server;
+
+/* Library ------------------------------------------------------------------ */
+const char *eqd_last_error(void);
+const char *eqd_version(void);
+void eqd_default_opts(eqd_solve_opts *opts);
+int eqd_device_count(int32_t *count);
+
+/* Grid (the FaultElasticity analogue) -------------------------------------- */
+int eqd_grid_create(const eqd_grid_desc *desc, eqd_grid **out);
+int eqd_grid_destroy(eqd_grid *grid);
+/* ntot = 6 n1 n2 n3; nf = n2f * n3f (`frictional_node_count`, src/FaultResponse.jl:168). */
+int eqd_grid_info(const eqd_grid *grid, int64_t *ntot, int32_t *nf, int32_t *n2f, int32_t *n3f);
+/* Omega_f coordinates (`fault_grid_axes`, src/FaultResponse.jl:161). */
+int eqd_grid_fault_axes(const eqd_grid *grid, double *x2f, double *x3f);
+
+/* Operator hooks (test / adapter surface) ----------------------------------
+ * x, y: ncols reference-layout vectors.
+ * mode 0: y = A x          (A = -H P (D+SAT) P; `mul!(y, A, x)` on the
+ *                            assembled matrix of src/ElasticitySplitNode.jl:211)
+ * mode 1: y = HP_DSAT x    (= H P (D+SAT) x, the RHS operator of :210)
+ * precision: EQD_PREC_FP64 or EQD_PREC_MIXED (FP32 arithmetic). */
+int eqd_apply(eqd_grid *grid, const double *x, double *y, int32_t ncols, int32_t mode, int32_t precision);
+
+/* `split_node_solve(solver, rhs)` (src/ElasticitySplitNode.jl:378-396) on the
+ * matrix-free A: solves A u = rhs for ncols reference-layout right-hand
+ * sides; iters/status per column (may be NULL). FP64 only. */
+int eqd_cg_solve(eqd_grid *grid, const double *rhs, double *u, int32_t ncols, const eqd_solve_opts *opts,
+                 int32_t *iters, int8_t *status, eqd_stats *stats);
+
+/* `shear_traction(fe, s2, s3)` (src/FaultResponse.jl:194-211) for nslip slip
+ * distributions: s2, s3, dtau2, dtau3 are nf x nslip, column-major. */
+int eqd_shear_traction(eqd_grid *grid, const double *s2, const double *s3, int32_t nslip, double *dtau2,
+                       double *dtau3, const eqd_solve_opts *opts, eqd_stats *stats);
+
+/* `fault_stiffness(fe)` (src/FaultResponse.jl:229-287): the full 2nf x 2nf K
+ * into the caller's buffer (>= 8 (2nf)^2 bytes). */
+int eqd_stiffness_exact(eqd_grid *grid, const eqd_solve_opts *opts, double *K, eqd_stats *stats);
+
+/* A subset of K's columns (0-based indices) into out (2nf x ncols);
+ * iters / status per column may be NULL. Same column semantics as above. */
+int eqd_stiffness_columns(eqd_grid *grid, const int32_t *cols, int32_t ncols, const eqd_solve_opts *opts,
+                          double *out, int32_t *iters, int8_t *status, eqd_stats *stats);
+
+/* Same as eqd_stiffness_columns, but `out_device` is a DEVICE pointer (on the
+ * grid's device, 2nf x ncols FP64, column-major): K stays resident in HBM,
+ * for device-side consumers (CuArray / torch). Returns when the columns are
+ * written. */
+int eqd_stiffness_columns_device(eqd_grid *grid, const int32_t *cols, int32_t ncols, const eqd_solve_opts *opts,
+                                 double *out_device, int32_t *iters, int8_t *status, eqd_stats *stats);
+
+/* `fault_stiffness_toeplitz(fe)` (src/FaultResponse.jl:339-393): 10 solves
+ * (centre then the 4 corners, first source wins), expanded on the device. */
+int eqd_stiffness_toeplitz(eqd_grid *grid, const eqd_solve_opts *opts, double *K, eqd_stats *stats);
+
+/* Measurement hook: times `reps` launches of the stencil apply y = A x on
+ * ncols device-resident random columns with CUDA events on the library's
+ * stream (after `warmup` untimed launches). precision: EQD_PREC_MIXED (FP32)
+ * or EQD_PREC_FP64. Writes the mean launch time (ms) and the algorithmic
+ * bytes of one launch (2 * Ntot * sizeof(T) * ncols). */
+int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t warmup, int32_t reps,
+                      double *ms_per_launch, double *bytes_per_launch);
+
+/* Jacobi diagonal, `diag(A)` (src/ElasticitySplitNode.jl:352-357), reference layout. */
+int eqd_diag(eqd_grid *grid, double *d);
+
+/* Time-loop GEMV `mul!(Δτ, K, slip)` (src/BP8.jl:366) ----------------------
+ * K stays resident on the device; y = K s for nvec vectors (n x nvec each). */
+int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out);
+int eqd_kmat_gemv(eqd_kmat *kmat, const double *s, double *y, int32_t nvec);
+int eqd_kmat_destroy(eqd_kmat *kmat);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EQD_H */

@@ -1,0 +1,150 @@
+"""GPU fault stiffness against the oracle, plus the reference's own K tests
+(test/fault_response_test.jl, test/bp8_test.jl:27-37) run on the GPU path."""
+import numpy as np
+import pytest
+
+from oracle.fault import FaultElasticity as OracleFE, cube_grids, bp8_grids, lame_lambda
+from oracle.krylov_cg import krylov_cg
+from oracle.operators import SplitNodeSystem
+from oracle.cref import CRefStiffness
+
+pytestmark = pytest.mark.gpu
+
+LAM, MU = 2.0, 1.0
+K_TOL = 1e-8   # relative Frobenius error of K against the tight FP64 oracle
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def small(eqd):
+    """n = 11 cubes, l_f = 0.4: nf = 25, 50 columns (test/fault_response_test.jl:80-88)."""
+    gm, gp = cube_grids(11)
+    ofe = OracleFE(gm, gp, LAM, MU, l_f=0.4)
+    K_ref, it, ok = CRefStiffness(ofe).columns(np.arange(2 * ofe.nf), rtol=1e-13)
+    assert ok.all()
+    return ofe, K_ref
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_K_matches_oracle(eqd, small, precision):
+    ofe, K_ref = small
+    fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4, precision=precision)
+    K = eqd.fault_stiffness(fe)
+    assert K.shape == K_ref.shape
+    assert rel(K, K_ref) < K_TOL
+    assert abs(K - K_ref).max() / abs(K_ref).max() < K_TOL
+    r = eqd.elastic_solver_report(fe)
+    assert r["solves"] == 2 * fe.nf and r["unconverged"] == 0
+    assert (np.diag(K) < 0).all()
+
+
+def test_cg_solve_krylov_parity(eqd):
+    """split_node_solve on the Gaussian slip patch: same iteration count as
+    Krylov's rule on the assembled matrix (71 at n = 9, 108 at n = 13), same u."""
+    for n, want in ((9, 71), (13, 108)):
+        gm, gp = cube_grids(n)
+        S = SplitNodeSystem(gm, gp, LAM, MU)
+        chi = S.build_chi(lambda x2, x3: (np.exp(-(x2 ** 2 + x3 ** 2) / 0.125), 0.0))
+        b = S.HP_DSAT @ chi
+        u_ref, it_ref, _, _ = krylov_cg(S.A, b, 1e-10)
+        assert it_ref == want
+        fe = eqd.FaultElasticity(eqd.cube_grids(n), LAM, MU, 0.0, precision="fp64")
+        u = eqd.split_node_solve(fe.rs, b)
+        rep = eqd.solver_report(fe.rs)
+        assert abs(rep["iterations"] - want) <= 1, rep
+        assert rep["unconverged"] == 0
+        U, U_ref = S.reconstruct_U(u, chi), S.reconstruct_U(u_ref, chi)
+        assert rel(U, U_ref) < 1e-8
+        assert np.linalg.norm(b - S.A @ u) / np.linalg.norm(b) < 1e-8
+
+
+def test_reference_fault_response_suite(eqd):
+    """test/fault_response_test.jl:43-88 on the GPU path (n = 13, L = 1.2, l_f = 0.6)."""
+    fe = eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.6)
+    x2, x3 = eqd.fault_grid_axes(fe)
+    assert np.isclose(x2[0], -0.6) and np.isclose(x2[-1], 0.6)
+    assert fe.nf == len(x2) * len(x3)
+    with pytest.raises(ValueError):
+        eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.55)
+    K = eqd.fault_stiffness(fe)
+    nf = fe.nf
+    k = np.arange(1, nf + 1)
+    s2, s3 = 0.01 * np.sin(3 * k), 0.02 * np.cos(2 * k)
+    d2, d3 = eqd.shear_traction(fe, s2, s3)
+    st = K @ np.concatenate([s2, s3])
+    assert np.allclose(st[:nf], d2, rtol=1e-8) and np.allclose(st[nf:], d3, rtol=1e-8)
+    assert (np.diag(K) < 0).all()
+    d2, _ = eqd.shear_traction(fe, np.ones(nf), np.zeros(nf))
+    assert d2.max() < 0
+    z2, z3 = eqd.shear_traction(fe, np.zeros(nf), np.zeros(nf))
+    assert (z2 == 0).all() and (z3 == 0).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_equals_single(eqd, precision):
+    """A column computed in a batch is bit-identical to the same column alone
+    (the reference's `threaded K build matches serial`, :100-112)."""
+    fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4, precision=precision)
+    cols = np.arange(2 * fe.nf)
+    Kb, itb, stb = eqd.stiffness_columns(fe, cols)
+    for c in (0, 7, fe.nf + 3):
+        K1, it1, _ = eqd.stiffness_columns(fe, [c])
+        assert np.array_equal(K1[:, 0], Kb[:, c])
+        assert it1[0] == itb[c]
+    Kp, itp, _ = eqd.stiffness_columns(fe, cols[::-1])
+    assert np.array_equal(Kp[:, ::-1], Kb)
+
+
+def test_toeplitz(eqd, small):
+    """test/fault_response_test.jl:128-171."""
+    ofe, K_exact = small
+    fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4)
+    Kt = eqd.fault_stiffness_toeplitz(fe)
+    Kt_ref = ofe.fault_stiffness_toeplitz(
+        columns={c: K_exact[:, c] for c in range(2 * ofe.nf)})
+    assert rel(Kt, Kt_ref) < K_TOL
+    nf = fe.nf
+    n2, n3 = fe.n2f, fe.n3f
+    c = ((n3 + 1) // 2 - 1) * n2 + (n2 + 1) // 2 - 1
+    assert rel(Kt, K_exact) < 0.05
+    assert np.allclose(Kt[:nf, c], K_exact[:nf, c], rtol=1e-6)
+    assert np.allclose(Kt[nf:, nf + c], K_exact[nf:, nf + c], rtol=1e-6)
+    assert (np.diag(Kt)[:nf] < 0).all()
+    assert np.isclose(Kt[c, c], K_exact[c, c], rtol=1e-6)
+    assert not np.isclose(Kt[0, 0], K_exact[0, 0], rtol=1e-6)
+    assert np.isclose(Kt[0, 0], K_exact[0, 0], rtol=0.05)
+    assert eqd.solver_report(fe.rs)["solves"] == 10
+
+
+def test_bp8_dz100_model(eqd):
+    """The reference's BP8 test model (test/bp8_test.jl:14, 27-37): dz = 100,
+    L = (800, 800), l_f = 400 -> 17x17x9 per side; published max diag K
+    -2.19e8 and asymmetry 0.1827 %."""
+    m = eqd.build_model(dz=100.0, L_fault=800.0, L_normal=800.0, stiffness="exact")
+    K, nf = m["K"], m["nf"]
+    assert K.shape == (2 * nf, 2 * nf)
+    assert (np.diag(K) < 0).all()
+    assert np.linalg.norm(K - K.T) / np.linalg.norm(K) < 0.01
+    assert f"{np.diag(K).max():.2e}" == "-2.19e+08"
+    assert f"{100 * np.linalg.norm(K - K.T) / np.linalg.norm(K):.4f}" == "0.1827"
+    mu = 32.04e9
+    gm, gp = bp8_grids(100.0, 800.0, 800.0)
+    ofe = OracleFE(gm, gp, lame_lambda(mu, 0.25), mu, 400.0)
+    K_ref, _, ok = CRefStiffness(ofe).columns(np.arange(2 * nf), rtol=1e-13)
+    assert rel(K, K_ref) < K_TOL
+
+
+def test_gemv(eqd):
+    rng = np.random.default_rng(0)
+    n = 578
+    K = rng.standard_normal((n, n))
+    M = eqd.KMatrix(K)
+    s = rng.standard_normal(n)
+    y = M.gemv(s)
+    assert np.allclose(y, K @ s, rtol=1e-12, atol=1e-12 * abs(K).sum(1).max())
+    S = rng.standard_normal((n, 3))
+    Y = M.gemv(S)
+    assert np.allclose(Y, K @ S, rtol=1e-12, atol=1e-10)
