@@ -291,6 +291,18 @@ def main():
         C.c_void_p(kdev.data_ptr()), None, None, C.byref(st64)))
     batched64_v = len(cols) / st64.device_seconds
 
+    # Autotuner evidence: every FP32 launch variant timed on the batch.
+    sel = C.c_int32()
+    nv = C.c_int32()
+    tms = (C.c_double * 8)()
+    trows = (C.c_int32 * 8)()
+    tthr = (C.c_int32 * 8)()
+    eqd._abi.check(lib.eqd_autotune(fe.handle, C.c_int32(min(len(cols), 512)), C.byref(sel), tms, trows, tthr,
+                                    C.byref(nv)))
+    autotune = {"selected": sel.value,
+                "variants": [{"tile_rows": trows[i], "threads": tthr[i], "ms_512_columns": tms[i]}
+                             for i in range(nv.value)]}
+
     # Roofline of the dominant kernel: FP32 stencil apply over the batch.
     ms = C.c_double()
     by = C.c_double()
@@ -340,6 +352,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": "plane_march_kernel<float,MODE_A>",
                      "peak_kind": peak_kind},
+        "autotune": autotune,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,

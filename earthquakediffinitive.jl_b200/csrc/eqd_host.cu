@@ -67,22 +67,25 @@ struct MarchCfg {
     size_t smem = 0;
 };
 
-static constexpr int kMaxT32 = 640;
+static constexpr int kMaxT32 = 640;   // generic FP32 instances
+static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register spills
 static constexpr int kMaxT64 = 384;
+static constexpr int kNumVariants = 3;
 
 template <typename T>
 static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, int maxt, int tile_rows,
                            const GridConst &gc, MarchCfg &out, std::string &why) {
     const int per_row = 2 * n1;
-    int t2 = tile_rows > 0 ? tile_rows : maxt / per_row;
+    int t2 = tile_rows > 0 ? std::min(tile_rows, maxt / per_row) : maxt / per_row;
     t2 = std::min(t2, n2);
     if (t2 * per_row > maxt) t2 = maxt / per_row;
     int ntiles = (n2 + t2 - 1) / t2;
     if (ntiles < 1) ntiles = 1;
-    // Balanced tiles, every tile at least 6 rows (closure reach of the wide operator).
-    while (ntiles > 1 && n2 / ntiles < 6) --ntiles;
+    // Balanced tiles, every tile at least 7 rows: the wide operator's closure
+    // rows reach 10 rows in from the boundary, and a tile reads 4 halo rows.
+    while (ntiles > 1 && n2 / ntiles < 7) --ntiles;
     const int t2max = (n2 + ntiles - 1) / ntiles;
-    if (t2max * per_row > maxt || n2 / ntiles < std::min(6, n2)) {
+    if (t2max * per_row > maxt || n2 / ntiles < std::min(7, n2)) {
         why = "grid too large in x1 for one CTA (n1=" + std::to_string(n1) + ")";
         return false;
     }
@@ -105,8 +108,8 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     int threads = per_row * t2max;
     threads = (threads + 31) / 32 * 32;
     out.threads = threads;
-    out.smem = 64 + 32 * 8 + (size_t)EQD_NSLOT * 6 * CH * sizeof(T) + 2 * (size_t)threads * sizeof(T) +
-               2 * (size_t)t2max * 6 * sizeof(T);
+    // barriers + flags, reduction scratch, plane ring, F1/H21 exchange [2][points] x 2
+    out.smem = 64 + 32 * 8 + (size_t)EQD_NSLOT * 6 * CH * sizeof(T) + 4 * (size_t)(2 * n1 * t2max) * sizeof(T);
     return true;
 }
 
@@ -132,7 +135,7 @@ struct Workspace {
     DevBuf active;
     int *h_active = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_cap = -1, graph_prec = -1, graph_iters = 0, graph_generic = -1;
+    int graph_cap = -1, graph_prec = -1, graph_iters = 0, graph_generic = -1, graph_sel = -1;
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
         if (h_active) cudaFreeHost(h_active);
@@ -146,6 +149,12 @@ struct eqd_grid {
     OpConst<float> c32;
     OpConst<double> c64;
     MarchCfg m32, m64;
+    // FP32 A-apply launch variants (see make_variants) and the chosen one.
+    MarchCfg v32[kNumVariants];
+    int v32_maxt[kNumVariants] = {0, 0, 0};
+    int sel32 = 0;
+    bool tuned = false;
+    double tune_ms[kNumVariants] = {0, 0, 0};
     int nchunks = 1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -167,7 +176,23 @@ struct eqd_kmat {
 // Kernel launch helpers
 // ---------------------------------------------------------------------------
 template <typename T, typename TO, int MODE>
-static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols) {
+static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols,
+                                int variant = -1) {
+    if (sizeof(T) == 4 && MODE == MODE_A) {
+        const int v = variant >= 0 ? variant : G->sel32;
+        const MarchCfg &m = G->v32[v];
+        cs.ncols = ncols;
+        dim3 grid((unsigned)(ncols * m.g.ntiles));
+        const float *fin = reinterpret_cast<const float *>(in);
+        float *fout = reinterpret_cast<float *>(out);
+        if (G->v32_maxt[v] == kMaxT32)
+            plane_march_kernel<float, float, MODE_A, kMaxT32><<<grid, m.threads, m.smem, G->stream>>>(
+                G->c32, m.g, fin, fout, cs, partials, G->err.as<unsigned>());
+        else
+            plane_march_kernel<float, float, MODE_A, kMaxT32b><<<grid, m.threads, m.smem, G->stream>>>(
+                G->c32, m.g, fin, fout, cs, partials, G->err.as<unsigned>());
+        return cudaGetLastError();
+    }
     constexpr int MAXT = sizeof(T) == 4 ? kMaxT32 : kMaxT64;
     const MarchCfg &m = sizeof(T) == 4 ? G->m32 : G->m64;
     const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
@@ -183,6 +208,7 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
 static cudaError_t configure_kernels(int smem_max) {
     const void *ks[] = {
         (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32>,
+        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32b>,
         (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32>,
         (const void *)plane_march_kernel<float, float, MODE_RHS, kMaxT32>,
         (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64>,
@@ -306,15 +332,32 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT32, 0, gc, G->m32, why) ||
         !make_march_cfg<double>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT64, 0, gc, G->m64, why))
         return fail(EQD_ERR_ARG, why);
+    // FP32 A-apply variants: one large CTA per SM (640-thread bound, may
+    // spill), one CTA of up to 512 threads (no spill), and CTAs of up to 256
+    // threads so that two share an SM.
+    {
+        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256};
+        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b};
+        for (int v = 0; v < kNumVariants; ++v) {
+            G->v32_maxt[v] = mt[v];
+            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], 0, gc, G->v32[v], why)) {
+                G->v32[v] = G->m32;  // fall back to the generic configuration
+                G->v32_maxt[v] = kMaxT32;
+            }
+        }
+        G->sel32 = 1;
+    }
     G->nchunks = (int)std::max<long long>(1, (gc.colstride + 16383) / 16384);
 
     CUDA_OR_RETURN(cudaSetDevice(d->device));
     {
         int optin = 0;
         CUDA_OR_RETURN(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
-        if ((size_t)optin < std::max(G->m32.smem, G->m64.smem))
+        size_t need = std::max(G->m32.smem, G->m64.smem);
+        for (int v = 0; v < kNumVariants; ++v) need = std::max(need, G->v32[v].smem);
+        if ((size_t)optin < need)
             return fail(EQD_ERR_ARG, "stencil tile needs more shared memory than the device offers");
-        CUDA_OR_RETURN(configure_kernels((int)std::max(G->m32.smem, G->m64.smem)));
+        CUDA_OR_RETURN(configure_kernels((int)need));
     }
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
     CUDA_OR_RETURN(cudaEventCreate(&G->ev0));
@@ -404,6 +447,49 @@ extern "C" int eqd_apply(eqd_grid *G, const double *x, double *y, int32_t ncols,
 }
 
 // ---------------------------------------------------------------------------
+// Autotuning of the FP32 A-apply launch variant (once per grid): each variant
+// is timed on `ncols` device-resident columns; the fastest is kept. The
+// choice is fixed for the grid's lifetime, so every column of every later
+// call uses the same tile partition (and the same reduction order).
+// ---------------------------------------------------------------------------
+static int tune_variants(eqd_grid *G, int ncols) {
+    const GridConst &gc = G->gc;
+    ncols = std::max(ncols, 1);
+    DevBuf x, y, part;
+    const long long n = gc.colstride * (long long)ncols;
+    CUDA_OR_RETURN(x.ensure(sizeof(float) * n));
+    CUDA_OR_RETURN(y.ensure(sizeof(float) * n));
+    int ntmax = 1;
+    for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
+    CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * ntmax));
+    fill_random_kernel<float><<<1184, 256, 0, G->stream>>>(x.as<float>(), n, 777ull);
+    CUDA_OR_RETURN(cudaGetLastError());
+    ColumnSet cs{};
+    double best = 1e30;
+    int bestv = G->sel32;
+    for (int v = 0; v < kNumVariants; ++v) {
+        CUDA_OR_RETURN((launch_march<float, float, MODE_A>(G, x.as<float>(), y.as<float>(), cs, part.as<double>(),
+                                                            ncols, v)));
+        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+        for (int r = 0; r < 3; ++r)
+            CUDA_OR_RETURN((launch_march<float, float, MODE_A>(G, x.as<float>(), y.as<float>(), cs,
+                                                                part.as<double>(), ncols, v)));
+        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+        CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
+        float ms = 0.f;
+        CUDA_OR_RETURN(cudaEventElapsedTime(&ms, G->ev0, G->ev1));
+        G->tune_ms[v] = ms / 3.0;
+        if (G->tune_ms[v] < best) {
+            best = G->tune_ms[v];
+            bestv = v;
+        }
+    }
+    G->sel32 = bestv;
+    G->tuned = true;
+    return check_device_error(G);
+}
+
+// ---------------------------------------------------------------------------
 // Batched CG driver
 // ---------------------------------------------------------------------------
 struct BatchSpec {
@@ -488,14 +574,20 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
     if (rc) return rc;
     Workspace &W = G->ws;
     const size_t vec = (size_t)gc.colstride * chunk;
-    const int nt32 = G->m32.g.ntiles, nt64 = G->m64.g.ntiles;
+    if (mixed && !G->tuned) {
+        rc = tune_variants(G, std::min(chunk, 512));
+        if (rc) return rc;
+    }
+    const int nt32 = G->v32[G->sel32].g.ntiles, nt64 = G->m64.g.ntiles;
     const int ntA = sizeof(T) == 4 ? nt32 : nt64;
     CUDA_OR_RETURN(W.x64.ensure(sizeof(double) * vec));
     CUDA_OR_RETURN(W.v0.ensure(sizeof(T) * vec));
     CUDA_OR_RETURN(W.v1.ensure(sizeof(T) * vec));
     CUDA_OR_RETURN(W.v2.ensure(sizeof(T) * vec));
     if (mixed) CUDA_OR_RETURN(W.v3.ensure(sizeof(float) * vec));
-    CUDA_OR_RETURN(W.apply_part.ensure(sizeof(double) * 2 * chunk * std::max(nt32, nt64)));
+    int ntmax = std::max(nt64, G->m32.g.ntiles);
+    for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
+    CUDA_OR_RETURN(W.apply_part.ensure(sizeof(double) * 2 * chunk * ntmax));
     CUDA_OR_RETURN(W.res_part.ensure(sizeof(double) * 2 * chunk * std::max(nt64, G->nchunks)));
     CUDA_OR_RETURN(W.rr_part.ensure(sizeof(double) * chunk * G->nchunks));
     for (DevBuf *b : {&W.gamma, &W.beta, &W.rr_ref, &W.tol, &W.bnorm}) CUDA_OR_RETURN(b->ensure(sizeof(double) * chunk));
@@ -526,7 +618,8 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
 
     // Graph of a few iterations, captured once per (chunk, precision, mode).
     const int kIter = 10;
-    if (!W.graph || W.graph_cap != chunk || W.graph_prec != o.precision || W.graph_generic != generic) {
+    if (!W.graph || W.graph_cap != chunk || W.graph_prec != o.precision || W.graph_generic != generic ||
+        W.graph_sel != G->sel32) {
         if (W.graph) cudaGraphExecDestroy(W.graph);
         W.graph = nullptr;
         cudaGraph_t g;
@@ -540,6 +633,7 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
         W.graph_cap = chunk;
         W.graph_prec = o.precision;
         W.graph_generic = generic;
+        W.graph_sel = G->sel32;
         W.graph_iters = kIter;
     }
 
@@ -850,7 +944,12 @@ static int profile_apply_impl(eqd_grid *G, int ncols, int warmup, int reps, doub
     const long long n = gc.colstride * (long long)ncols;
     CUDA_OR_RETURN(x.ensure(sizeof(T) * n));
     CUDA_OR_RETURN(y.ensure(sizeof(T) * n));
-    const int nt = sizeof(T) == 4 ? G->m32.g.ntiles : G->m64.g.ntiles;
+    if (sizeof(T) == 4 && !G->tuned) {
+        int rc = tune_variants(G, std::min(ncols, 512));
+        if (rc) return rc;
+    }
+    int nt = G->m64.g.ntiles;
+    for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, G->v32[v].g.ntiles);
     CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * nt));
     fill_random_kernel<T><<<1184, 256, 0, G->stream>>>(x.as<T>(), n, 12345ull);
     CUDA_OR_RETURN(cudaGetLastError());
@@ -877,6 +976,23 @@ extern "C" int eqd_profile_apply(eqd_grid *G, int32_t ncols, int32_t precision, 
     if (precision == EQD_PREC_MIXED) return profile_apply_impl<float>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
     if (precision == EQD_PREC_FP64) return profile_apply_impl<double>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
     return fail(EQD_ERR_ARG, "unknown precision");
+}
+
+extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, double *ms_per_variant,
+                            int32_t *tile_rows, int32_t *threads, int32_t *nvariants) {
+    if (!G || ncols < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    int rc = tune_variants(G, ncols);
+    if (rc) return rc;
+    if (selected) *selected = G->sel32;
+    if (nvariants) *nvariants = kNumVariants;
+    for (int v = 0; v < kNumVariants; ++v) {
+        if (ms_per_variant) ms_per_variant[v] = G->tune_ms[v];
+        if (tile_rows) tile_rows[v] = G->v32[v].g.t2max;
+        if (threads) threads[v] = G->v32[v].threads;
+    }
+    return EQD_OK;
 }
 
 extern "C" int eqd_diag(eqd_grid *G, double *d) {

@@ -98,7 +98,7 @@ void fill_axis(AX &a, int n, double h) {
             a.d2_corrR[r][k] = (T)(in(cR) ? M.d2(rR, cR) - d2i(rR, cR) : 0.0);
         }
     for (int r = 0; r < 6; ++r)
-        for (int k = 0; k < 10; ++k) {
+        for (int k = 0; k < 11; ++k) {
             const int cL = k, rR = n - 1 - r, cR = n - 1 - k;
             a.w_corrL[r][k] = (T)(in(cL) ? M.w(r, cL) - wi(r, cL) : 0.0);
             a.w_corrR[r][k] = (T)(in(cR) ? M.w(rR, cR) - wi(rR, cR) : 0.0);

@@ -25,14 +25,22 @@
 // W_2 = D1_2 D1_2 (the wide operator, as a 1D matrix).
 //
 // Work decomposition (one CTA per (column, x2-tile)):
-//   * threads = both sides x all n1 points x the tile's x2 rows;
+//   * one thread per point of the tile: both sides x all n1 points x the
+//     tile's x2 rows, grouped into warp-uniform classes (x2-interior rows,
+//     x2-closure rows, fault nodes with the two sides in adjacent lanes);
 //   * x1 derivatives read the thread's own line from shared memory;
 //   * x2 derivatives read neighbouring rows (tile + 4-row halo) from shared;
-//   * x3 is marched plane by plane; x3 derivatives come from 7-deep register
-//     windows (closure rows reach +-3 planes);
+//   * x3 is marched plane by plane; x3 derivatives come from 7-slot register
+//     windows (closure rows reach +-3 planes), rotated by unrolling the march
+//     by 7 rather than by moving registers;
 //   * planes arrive through a 6-slot ring filled by cp.async.bulk copies
-//     completing on mbarriers, three planes ahead of use.
+//     completing on mbarriers, three planes ahead of use;
+//   * one CTA barrier per plane (the x1 exchange of F1/H21, double-buffered
+//     by step parity); the interface exchange between the two sides of a
+//     fault node is a lane shuffle.
 #pragma once
+#include <type_traits>
+
 #include "eqd_common.cuh"
 
 namespace eqd {
@@ -46,12 +54,14 @@ enum { MODE_A = 0, MODE_AP = 1, MODE_RHS = 2 };
 //                   n-1..n-4)
 //   *_corrL[r][k] : row r minus the interior stencil, columns k (lower end)
 //   *_corrR[r][k] : row n-1-r minus the interior stencil, columns n-1-k
+// (rows of the wide operator W span up to 11 columns: both closures reach
+// the middle row when n = 11)
 template <typename T>
 struct AxisT {
     T d1_int[5], d2_int[5], w_int[9];
     T d1_corrL[4][6], d1_corrR[4][6];
     T d2_corrL[4][6], d2_corrR[4][6];
-    T w_corrL[6][10], w_corrR[6][10];
+    T w_corrL[6][11], w_corrR[6][11];
     T d1_cl[8][7], d2_cl[8][7];
     T dlo[4];
     T wq[4];
@@ -74,92 +84,95 @@ struct MarchGeom {
     int i2f0, n2f, i3f0, n3f, nf;
 };
 
-// Out-of-range window entries are zero and meet zero coefficients.
-template <typename T>
-__device__ __forceinline__ T x3_d1(const OpConst<T> &C, const T (&w)[7], int q, int n3) {
-    const AxisT<T> &a = C.ax[2];
+// x3 derivatives from a 7-slot register window in which plane q lives in
+// slot q % 7; C0 is the (compile-time) slot of the centre plane q. Planes
+// outside the domain hold zero and meet zero coefficients.
+template <int C0, typename T>
+__device__ __forceinline__ T x3_d1(const AxisT<T> &a, const T (&w)[7], int q, int n3) {
     if (q >= 4 && q <= n3 - 5)
-        return a.d1_int[0] * w[1] + a.d1_int[1] * w[2] + a.d1_int[3] * w[4] + a.d1_int[4] * w[5];
+        return a.d1_int[0] * w[(C0 + 5) % 7] + a.d1_int[1] * w[(C0 + 6) % 7] + a.d1_int[3] * w[(C0 + 1) % 7] +
+               a.d1_int[4] * w[(C0 + 2) % 7];
     const int r = q < 4 ? q : 4 + (n3 - 1 - q);
     T s = T(0);
 #pragma unroll
-    for (int o = 0; o < 7; ++o) s += a.d1_cl[r][o] * w[o];
+    for (int o = -3; o <= 3; ++o) s += a.d1_cl[r][o + 3] * w[(C0 + o + 7) % 7];
     return s;
 }
 
-template <typename T>
-__device__ __forceinline__ T x3_d2(const OpConst<T> &C, const T (&w)[7], int q, int n3) {
-    const AxisT<T> &a = C.ax[2];
+template <int C0, typename T>
+__device__ __forceinline__ T x3_d2(const AxisT<T> &a, const T (&w)[7], int q, int n3) {
     if (q >= 4 && q <= n3 - 5)
-        return a.d2_int[0] * w[1] + a.d2_int[1] * w[2] + a.d2_int[2] * w[3] + a.d2_int[3] * w[4] +
-               a.d2_int[4] * w[5];
+        return a.d2_int[0] * w[(C0 + 5) % 7] + a.d2_int[1] * w[(C0 + 6) % 7] + a.d2_int[2] * w[C0] +
+               a.d2_int[3] * w[(C0 + 1) % 7] + a.d2_int[4] * w[(C0 + 2) % 7];
     const int r = q < 4 ? q : 4 + (n3 - 1 - q);
     T s = T(0);
 #pragma unroll
-    for (int o = 0; o < 7; ++o) s += a.d2_cl[r][o] * w[o];
+    for (int o = -3; o <= 3; ++o) s += a.d2_cl[r][o + 3] * w[(C0 + o + 7) % 7];
     return s;
-}
-
-template <typename T>
-__device__ __forceinline__ void shift7(T (&w)[7], T v) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) w[k] = w[k + 1];
-    w[6] = v;
 }
 
 // x2-direction D1 / D2 / W at row r of a chunk pointer `c` (own element),
-// row stride n1. Interior stencil everywhere (rows beyond the domain read
-// zeros), plus the closure correction on the first/last rows.
+// row stride n1: the interior stencil everywhere (rows beyond the domain read
+// zeros) plus, for closure rows (`cl`), the closure correction.
 template <typename T>
-__device__ __forceinline__ T x2_d1(const AxisT<T> &a, const T *c, int n1, int r, int n2) {
+__device__ __forceinline__ T x2_d1(const AxisT<T> &a, const T *c, int n1, int r, int n2, bool cl) {
     T s = a.d1_int[0] * c[-2 * n1] + a.d1_int[1] * c[-n1] + a.d1_int[3] * c[n1] + a.d1_int[4] * c[2 * n1];
-    if (r < 4) {
-        const T *b = c - r * n1;
+    if (cl) {
+        if (r < 4) {
+            const T *b = c - r * n1;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s += a.d1_corrL[r][k] * b[k * n1];
-    } else if (r >= n2 - 4) {
-        const int rr = n2 - 1 - r;
-        const T *b = c + rr * n1;
+            for (int k = 0; k < 6; ++k) s += a.d1_corrL[r][k] * b[k * n1];
+        } else if (r >= n2 - 4) {
+            const int rr = n2 - 1 - r;
+            const T *b = c + rr * n1;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s += a.d1_corrR[rr][k] * b[-k * n1];
+            for (int k = 0; k < 6; ++k) s += a.d1_corrR[rr][k] * b[-k * n1];
+        }
     }
     return s;
 }
 
 template <typename T>
-__device__ __forceinline__ T x2_d2(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2) {
+__device__ __forceinline__ T x2_d2(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2, bool cl) {
     T s = a.d2_int[0] * c[-2 * n1] + a.d2_int[1] * c[-n1] + a.d2_int[2] * self + a.d2_int[3] * c[n1] +
           a.d2_int[4] * c[2 * n1];
-    if (r < 4) {
-        const T *b = c - r * n1;
+    if (cl) {
+        if (r < 4) {
+            const T *b = c - r * n1;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s += a.d2_corrL[r][k] * b[k * n1];
-    } else if (r >= n2 - 4) {
-        const int rr = n2 - 1 - r;
-        const T *b = c + rr * n1;
+            for (int k = 0; k < 6; ++k) s += a.d2_corrL[r][k] * b[k * n1];
+        } else if (r >= n2 - 4) {
+            const int rr = n2 - 1 - r;
+            const T *b = c + rr * n1;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s += a.d2_corrR[rr][k] * b[-k * n1];
+            for (int k = 0; k < 6; ++k) s += a.d2_corrR[rr][k] * b[-k * n1];
+        }
     }
     return s;
 }
 
 template <typename T>
-__device__ __forceinline__ T x2_w(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2) {
+__device__ __forceinline__ T x2_w(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2, bool cl) {
     T s = a.w_int[4] * self;
 #pragma unroll
     for (int o = 1; o <= 4; ++o) s += a.w_int[4 - o] * c[-o * n1] + a.w_int[4 + o] * c[o * n1];
-    if (r < 6) {
-        const T *b = c - r * n1;
+    if (cl) {
+        if (r < 6) {
+            const T *b = c - r * n1;
 #pragma unroll
-        for (int k = 0; k < 10; ++k) s += a.w_corrL[r][k] * b[k * n1];
-    } else if (r >= n2 - 6) {
-        const int rr = n2 - 1 - r;
-        const T *b = c + rr * n1;
+            for (int k = 0; k < 11; ++k) s += a.w_corrL[r][k] * b[k * n1];
+        } else if (r >= n2 - 6) {
+            const int rr = n2 - 1 - r;
+            const T *b = c + rr * n1;
 #pragma unroll
-        for (int k = 0; k < 10; ++k) s += a.w_corrR[rr][k] * b[-k * n1];
+            for (int k = 0; k < 11; ++k) s += a.w_corrR[rr][k] * b[-k * n1];
+        }
     }
     return s;
 }
+
+template <int V>
+using IC = std::integral_constant<int, V>;
 
 template <typename T, typename TO, int MODE, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
@@ -187,21 +200,54 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw);
+    volatile int *s_dead = reinterpret_cast<volatile int *>(smem_raw + 56);  // [2], by step parity
     double *red = reinterpret_cast<double *>(smem_raw + 64);
     T *ring = reinterpret_cast<T *>(smem_raw + 64 + 32 * 8);
-    const int NT = blockDim.x;
-    T *xF1 = ring + (size_t)EQD_NSLOT * 6 * g.CH;
-    T *xH21 = xF1 + NT;
-    T *face = xH21 + NT;  // [2][t2max][6]
+    const int NP = 2 * n1 * g.t2max;  // points per tile
+    T *xF1 = ring + (size_t)EQD_NSLOT * 6 * g.CH;  // [2][NP], by step parity
+    T *xH21 = xF1 + 2 * NP;                        // [2][NP]
 
+    // ---- thread -> point: warp-homogeneous classes --------------------------
+    // class 0: x2-interior rows, not on the fault; class 1: x2-closure rows,
+    // not on the fault; class 2: fault nodes, the two sides of a node in
+    // adjacent lanes (partners exchange by shuffle).
     const int tid = threadIdx.x;
-    const int per_side = n1 * g.t2max;
-    const int side = tid / per_side;
-    const int rem = tid - side * per_side;
-    const int i2l = rem / n1;
-    const int i1 = rem - i2l * n1;
-    const int i2 = a0 + i2l;
-    const bool valid = (side < 2) && (i2 < a1);
+    const int T2 = a1 - a0;
+    const int ilo = min(max(a0, 6), a1);
+    const int ihi = max(min(a1, n2 - 6), ilo);
+    const int nI = ihi - ilo;
+    const int per = 2 * (n1 - 1);
+    const int N0 = nI * per, N1 = (T2 - nI) * per, N2 = 2 * T2;
+    int side = 0, i2 = a0, i1 = 0, cls = 3;
+    if (tid < N0) {
+        const int rr = tid / per, q = tid % per;
+        side = q / (n1 - 1);
+        const int j = q % (n1 - 1);
+        i1 = side == 0 ? j : j + 1;
+        i2 = ilo + rr;
+        cls = 0;
+    } else if (tid < N0 + N1) {
+        const int k = tid - N0;
+        const int rr = k / per, q = k % per;
+        side = q / (n1 - 1);
+        const int j = q % (n1 - 1);
+        i1 = side == 0 ? j : j + 1;
+        const int nlow = ilo - a0;
+        i2 = rr < nlow ? a0 + rr : ihi + (rr - nlow);
+        cls = 1;
+    } else if (tid < N0 + N1 + N2) {
+        const int k = tid - N0 - N1;
+        side = k & 1;
+        i1 = side == 0 ? n1 - 1 : 0;
+        i2 = a0 + (k >> 1);
+        cls = 2;
+    }
+    const bool valid = cls < 3;
+    const bool is_face = cls == 2;
+    const bool x2cl = cls != 0 && (i2 < 6 || i2 >= n2 - 6);
+    const unsigned facemask = __ballot_sync(0xffffffffu, is_face);
+    const int i2l = i2 - a0;
+    const int pidx = (side * g.t2max + i2l) * n1 + i1;
 
     const T *incol = in + (long long)col * g.colstride;
     TO *outcol = out + (long long)col * g.colstride;
@@ -209,10 +255,12 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     // Zero the ring (rows outside the domain must read as zero), init barriers.
     {
         const int nring = EQD_NSLOT * 6 * g.CH;
-        for (int i = tid; i < nring; i += NT) ring[i] = T(0);
+        for (int i = tid; i < nring; i += blockDim.x) ring[i] = T(0);
         fence_proxy_async_smem();
         if (tid == 0) {
             for (int k = 0; k < EQD_NSLOT; ++k) mbar_init(&mbar[k], 1);
+            s_dead[0] = 0;
+            s_dead[1] = 0;
             fence_mbar_init();
         }
     }
@@ -227,20 +275,22 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             bulk_g2s(dst, src, bytes, &mbar[slot]);
         }
     };
-    int issued = min(EQD_NSLOT, n3), dead_at = 0;
+    int issued = min(EQD_NSLOT, n3);
     if (tid == 0) {
         for (int q = 0; q < issued; ++q) issue_plane(q);
     }
 
     // Per-thread x1 row operators (start column within the line + 6 taps).
     const AxisT<T> &A1 = C.ax[0];
+    const AxisT<T> &A2 = C.ax[1];
+    const AxisT<T> &A3 = C.ax[2];
     int s1;
     T c1[6], c2[6];
     if (i1 < 4) {
         s1 = 0;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const int o = k - i1;  // offset from the row
+            const int o = k - i1;
             c1[k] = (o >= -3 && o <= 3) ? A1.d1_cl[i1][o + 3] : T(0);
             c2[k] = (o >= -3 && o <= 3) ? A1.d2_cl[i1][o + 3] : T(0);
         }
@@ -256,45 +306,49 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     } else {
         s1 = i1 - 2;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) { c1[k] = A1.d1_int[k]; c2[k] = A1.d2_int[k]; }
+        for (int k = 0; k < 5; ++k) {
+            c1[k] = A1.d1_int[k];
+            c2[k] = A1.d2_int[k];
+        }
         c1[5] = T(0);
         c2[5] = T(0);
     }
-    const bool is_face = valid && ((side == 0 && i1 == n1 - 1) || (side == 1 && i1 == 0));
     const bool ff_x12 = (side == 0 && i1 == 0) || (side == 1 && i1 == n1 - 1) || i2 == 0 || i2 == n2 - 1;
     const T wq1 = (i1 < 4) ? A1.wq[i1] : (i1 >= n1 - 4 ? A1.wq[n1 - 1 - i1] : T(1));
-    const T wq2 = (i2 < 4) ? C.ax[1].wq[i2] : (i2 >= n2 - 4 ? C.ax[1].wq[n2 - 1 - i2] : T(1));
-    const double hpt = C.hvol * (double)wq1 * (double)wq2 * (MODE == MODE_RHS ? 1.0 : -1.0);
+    const T wq2 = (i2 < 4) ? A2.wq[i2] : (i2 >= n2 - 4 ? A2.wq[n2 - 1 - i2] : T(1));
+    const T hpt = (T)(C.hvol * (double)wq1 * (double)wq2 * (MODE == MODE_RHS ? 1.0 : -1.0));
 
-    const int own = i2 * n1 + i1 - base;                   // offset inside a chunk
-    const int lineoff = i2 * n1 + s1 - base;               // x1 window start
-    const int fidx = (side * g.t2max + i2l) * 6;           // my face record
-    const int oidx = ((1 - side) * g.t2max + i2l) * 6;     // partner's face record
-    const long long ooff = (long long)i2 * n1 + i1;        // plane offset in global
+    const int own = i2 * n1 + i1 - base;      // offset inside a chunk
+    const int lineoff = i2 * n1 + s1 - base;  // x1 window start
+    const long long ooff = (long long)i2 * n1 + i1;
 
-    T v1w[7], v2w[7], v3w[7], F3w[7], H23w[7], w3q[3];
+    T v1w[7], v2w[7], v3w[7], F3w[7], H23w[7], w3q[7];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) { v1w[k] = v2w[k] = v3w[k] = F3w[k] = H23w[k] = T(0); }
-    w3q[0] = w3q[1] = w3q[2] = T(0);
+    for (int k = 0; k < 7; ++k) v1w[k] = v2w[k] = v3w[k] = F3w[k] = H23w[k] = w3q[k] = T(0);
 
     double acc0 = 0.0, acc1 = 0.0;
-    bool dead = false;
+    const T lam = C.lam, mu = C.mu, lpm = C.lpm, sat = C.sat_c;
+    const int nsteps = n3 + 6;
+    int dead_at = -1;
 
-    const T lam = C.lam, mu = C.mu, lpm = C.lpm;
-    const AxisT<T> &A2 = C.ax[1];
-
-    for (int s = 0; s < n3 + 6; ++s) {
-        // ---- ingest plane s -------------------------------------------------
+    // One march step. Plane q of every window lives in slot q % 7; the step
+    // index modulo 7 is a compile-time constant R.
+    auto step = [&](auto Rc, int s) -> bool {
+        constexpr int R = decltype(Rc)::value;
+        constexpr int CP = (R + 4) % 7;  // slot of p = s - 3
+        constexpr int CZ = (R + 1) % 7;  // slot of z = s - 6
+        const int buf = s & 1;
+        // ---- ingest plane s ----------------------------------------------------
         if (s < n3) {
             const int slot = s % EQD_NSLOT;
-            if (!mbar_wait_bounded(&mbar[slot], (unsigned)((s / EQD_NSLOT) & 1), err)) dead = true;
+            if (!mbar_wait_bounded(&mbar[slot], (unsigned)((s / EQD_NSLOT) & 1), err)) s_dead[buf] = 1;
             if (MODE != MODE_A) {
                 // Fix-up pass on the landed plane: chi (RHS) or P (generic input).
                 T *pl = ring + (size_t)slot * 6 * g.CH;
                 const int nrows = r1 - r0;
                 if (MODE == MODE_RHS) {
                     if (s >= g.i3f0 && s < g.i3f0 + g.n3f) {
-                        for (int w = tid; w < nrows; w += NT) {
+                        for (int w = tid; w < nrows; w += blockDim.x) {
                             const int r = r0 + w;
                             if (r < g.i2f0 || r >= g.i2f0 + g.n2f) continue;
                             const int k = (r - g.i2f0) + g.n2f * (s - g.i3f0);
@@ -313,54 +367,46 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                     }
                 } else {  // MODE_AP: v = P x
                     const bool plane_ff = (s == 0 || s == n3 - 1);
-                    for (int w = tid; w < nrows * 3; w += NT) {
+                    for (int w = tid; w < nrows * 3; w += blockDim.x) {
                         const int r = r0 + w / 3, j = w % 3;
                         T *m = pl + (0 * 3 + j) * g.CH + r * n1 - base;
-                        T *p = pl + (1 * 3 + j) * g.CH + r * n1 - base;
+                        T *pp = pl + (1 * 3 + j) * g.CH + r * n1 - base;
                         if (plane_ff || r == 0 || r == n2 - 1) {
-                            for (int i = 0; i < n1; ++i) { m[i] = T(0); p[i] = T(0); }
+                            for (int i = 0; i < n1; ++i) {
+                                m[i] = T(0);
+                                pp[i] = T(0);
+                            }
                         } else {
                             m[0] = T(0);
-                            p[n1 - 1] = T(0);
-                            const T avg = T(0.5) * (m[n1 - 1] + p[0]);
+                            pp[n1 - 1] = T(0);
+                            const T avg = T(0.5) * (m[n1 - 1] + pp[0]);
                             m[n1 - 1] = avg;
-                            p[0] = avg;
+                            pp[0] = avg;
                         }
                     }
                 }
                 fence_proxy_async_smem();
                 __syncthreads();
             }
-            if (__syncthreads_or(dead)) {
-                dead = true;
-                dead_at = s;
-                break;
-            }
-            const T *pl = ring + (size_t)slot * 6 * g.CH;
-            const T *c3 = pl + (side * 3 + 2) * g.CH + own;
-            T a = T(0), b = T(0), c = T(0), h = T(0);
             if (valid) {
-                a = pl[(side * 3 + 0) * g.CH + own];
-                b = pl[(side * 3 + 1) * g.CH + own];
-                c = c3[0];
-                h = x2_d1(A2, c3, n1, i2, n2);
+                const T *pl = ring + (size_t)slot * 6 * g.CH;
+                const T *c3 = pl + (side * 3 + 2) * g.CH + own;
+                v1w[R] = pl[(side * 3 + 0) * g.CH + own];
+                v2w[R] = pl[(side * 3 + 1) * g.CH + own];
+                v3w[R] = c3[0];
+                H23w[R] = x2_d1(A2, c3, n1, i2, n2, x2cl);
+            } else {
+                v1w[R] = v2w[R] = v3w[R] = H23w[R] = T(0);
             }
-            shift7(v1w, a);
-            shift7(v2w, b);
-            shift7(v3w, c);
-            shift7(H23w, h);
         } else {
-            shift7(v1w, T(0));
-            shift7(v2w, T(0));
-            shift7(v3w, T(0));
-            shift7(H23w, T(0));
+            v1w[R] = v2w[R] = v3w[R] = H23w[R] = T(0);
         }
 
         // ---- in-plane work at p = s - 3 ---------------------------------------
         const int p = s - 3;
+        const bool pin = p >= 0 && p < n3;
         T w1 = T(0), w2 = T(0), w3p = T(0), F3 = T(0);
-        T tau1 = T(0), tau2 = T(0), tau3 = T(0);
-        if (p >= 0 && p < n3 && valid) {
+        if (valid && pin) {
             const T *pl = ring + (size_t)(p % EQD_NSLOT) * 6 * g.CH;
             const T *l1 = pl + (side * 3 + 0) * g.CH + lineoff;
             const T *l2 = pl + (side * 3 + 1) * g.CH + lineoff;
@@ -368,8 +414,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             const T *o1 = pl + (side * 3 + 0) * g.CH + own;
             const T *o2 = pl + (side * 3 + 1) * g.CH + own;
             const T *o3 = pl + (side * 3 + 2) * g.CH + own;
-            const T v1 = v1w[3], v2 = v2w[3], v3 = v3w[3];
-            // x1 direction: G1 and D2_1 of each component, boundary derivatives.
+            const T v1 = v1w[CP], v2 = v2w[CP], v3 = v3w[CP];
             T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
@@ -379,31 +424,28 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 A21 += c2[k] * x2;
                 A31 += c2[k] * x3;
             }
-            // x2 direction.
-            const T G2 = x2_d1(A2, o2, n1, i2, n2);
-            const T H21 = x2_d1(A2, o1, n1, i2, n2);
-            const T A12 = x2_d2(A2, o1, v1, n1, i2, n2);
-            const T A22 = x2_d2(A2, o2, v2, n1, i2, n2);
-            const T A32 = x2_d2(A2, o3, v3, n1, i2, n2);
-            const T W2 = x2_w(A2, o2, v2, n1, i2, n2);
-            // x3 direction (register windows centred on p).
-            const T G3 = x3_d1(C, v3w, p, n3);
-            const T A13 = x3_d2(C, v1w, p, n3);
-            const T A23 = x3_d2(C, v2w, p, n3);
-            const T A33 = x3_d2(C, v3w, p, n3);
-            const T D3H23 = x3_d1(C, H23w, p, n3);
-
+            const T G2 = x2_d1(A2, o2, n1, i2, n2, x2cl);
+            const T H21 = x2_d1(A2, o1, n1, i2, n2, x2cl);
+            const T A12 = x2_d2(A2, o1, v1, n1, i2, n2, x2cl);
+            const T A22 = x2_d2(A2, o2, v2, n1, i2, n2, x2cl);
+            const T A32 = x2_d2(A2, o3, v3, n1, i2, n2, x2cl);
+            const T W2 = x2_w(A2, o2, v2, n1, i2, n2, x2cl);
+            const T G3 = x3_d1<CP>(A3, v3w, p, n3);
+            const T A13 = x3_d2<CP>(A3, v1w, p, n3);
+            const T A23 = x3_d2<CP>(A3, v2w, p, n3);
+            const T A33 = x3_d2<CP>(A3, v3w, p, n3);
+            const T D3H23 = x3_d1<CP>(A3, H23w, p, n3);
             const T F1 = lam * G1 + lpm * (G2 + G3);
             F3 = lam * G3 + lpm * (G1 + G2);
-            xF1[tid] = F1;
-            xH21[tid] = H21;
             w1 = mu * (T(2) * A11 + A12 + A13);
             w2 = mu * (A21 + T(2) * A22 + A23) + lam * W2 + lpm * D3H23;
             w3p = mu * (A31 + A32 + T(2) * A33);
             if (is_face) {
-                // +x1 boundary derivative at the fault node: lower end of the
+                // Traction on the fixed +x1 axis (`traction_blocks`), with the
+                // +x1 boundary derivative of the fault node: lower end of the
                 // plus block (window cols 0..3), upper end of the minus block
-                // (window cols 5..2, odd mirror).
+                // (window cols 5..2, odd mirror). SAT c (tau^+ - tau^-) on both
+                // faces; the partner (other side) is the adjacent lane.
                 T dh1 = T(0), dh2 = T(0), dh3 = T(0);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -413,109 +455,110 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                     dh2 += cf * l2[q];
                     dh3 += cf * l3[q];
                 }
-                const T D3v1 = x3_d1(C, v1w, p, n3);
-                tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
-                tau2 = mu * (H21 + dh2);
-                tau3 = mu * (D3v1 + dh3);
-                face[fidx + 0] = tau1;
-                face[fidx + 1] = tau2;
-                face[fidx + 2] = tau3;
-            }
-        }
-        __syncthreads();
-        if (p >= 0 && p < n3 && valid) {
-            const int lb = tid - i1 + s1;  // x1 window start in the exchange arrays
-            T E1 = T(0), E21 = T(0);
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                E1 += c1[k] * xF1[lb + k];
-                E21 += c1[k] * xH21[lb + k];
-            }
-            w1 += E1;
-            w2 += lpm * E21;
-            if (is_face) {
-                // SAT: c (tau^+ - tau^-), added on both faces.
+                const T D3v1 = x3_d1<CP>(A3, v1w, p, n3);
+                const T tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
+                const T tau2 = mu * (H21 + dh2);
+                const T tau3 = mu * (D3v1 + dh3);
+                const T o1t = __shfl_xor_sync(facemask, tau1, 1);
+                const T o2t = __shfl_xor_sync(facemask, tau2, 1);
+                const T o3t = __shfl_xor_sync(facemask, tau3, 1);
                 const T sgn = side == 0 ? T(-1) : T(1);
-                w1 += C.sat_c * sgn * (tau1 - face[oidx + 0]);
-                w2 += C.sat_c * sgn * (tau2 - face[oidx + 1]);
-                w3p += C.sat_c * sgn * (tau3 - face[oidx + 2]);
+                w1 += sat * sgn * (tau1 - o1t);
+                w2 += sat * sgn * (tau2 - o2t);
+                w3p += sat * sgn * (tau3 - o3t);
             }
+            xF1[buf * NP + pidx] = F1;
+            xH21[buf * NP + pidx] = H21;
         }
-        // Queue w3's partial (needs D1_3 F3 three planes later), window F3.
-        const T w3z_part = w3q[0];
-        w3q[0] = w3q[1];
-        w3q[1] = w3q[2];
-        w3q[2] = w3p;
-        shift7(F3w, F3);
-        const int z = s - 6;
-        T w3 = T(0);
-        if (z >= 0 && z < n3 && valid) w3 = w3z_part + x3_d1(C, F3w, z, n3);
-        if (is_face) {
-            face[fidx + 3] = w1;
-            face[fidx + 4] = w2;
-            face[fidx + 5] = w3;
-        }
+        F3w[CP] = F3;
+        w3q[CP] = w3p;
         __syncthreads();
-
-        // ---- epilogue: P, H, store, dot partials ------------------------------
-        if (valid) {
-            if (p >= 0 && p < n3) {
-                const bool ff = ff_x12 || p == 0 || p == n3 - 1;
-                const int rq = p < 4 ? p : (p >= n3 - 4 ? n3 - 1 - p : -1);
-                const double hw = hpt * (rq >= 0 ? (double)C.ax[2].wq[rq] : 1.0);
-                double y1 = 0.0, y2 = 0.0;
-                if (!ff) {
-                    T u1 = w1, u2 = w2;
-                    if (is_face) {
-                        u1 = T(0.5) * (w1 + face[oidx + 3]);
-                        u2 = T(0.5) * (w2 + face[oidx + 4]);
-                    }
-                    y1 = hw * (double)u1;
-                    y2 = hw * (double)u2;
-                }
-                const long long o = ((long long)(side * 3 + 0) * n3 + p) * g.PS + ooff;
-                outcol[o] = (TO)y1;
-                outcol[o + (long long)n3 * g.PS] = (TO)y2;
-                if (MODE == MODE_RHS) {
-                    acc0 += (double)(TO)y1 * (double)(TO)y1 + (double)(TO)y2 * (double)(TO)y2;
-                } else {
-                    acc0 += (double)v1w[3] * (double)(TO)y1 + (double)v2w[3] * (double)(TO)y2;
-                    acc1 += (double)v1w[3] * (double)v1w[3] + (double)v2w[3] * (double)v2w[3];
-                }
-            }
-            if (z >= 0 && z < n3) {
-                const bool ff = ff_x12 || z == 0 || z == n3 - 1;
-                const int rq = z < 4 ? z : (z >= n3 - 4 ? n3 - 1 - z : -1);
-                const double hw = hpt * (rq >= 0 ? (double)C.ax[2].wq[rq] : 1.0);
-                double y3 = 0.0;
-                if (!ff) {
-                    T u3 = w3;
-                    if (is_face) u3 = T(0.5) * (w3 + face[oidx + 5]);
-                    y3 = hw * (double)u3;
-                }
-                const long long o = ((long long)(side * 3 + 2) * n3 + z) * g.PS + ooff;
-                outcol[o] = (TO)y3;
-                if (MODE == MODE_RHS) {
-                    acc0 += (double)(TO)y3 * (double)(TO)y3;
-                } else {
-                    acc0 += (double)v3w[0] * (double)(TO)y3;
-                    acc1 += (double)v3w[0] * (double)v3w[0];
-                }
-            }
+        if (s_dead[buf]) {
+            dead_at = s;
+            return false;
         }
-        // Slot of plane p is free once every thread passed the barrier above.
+        // Slot of plane p is free: every thread has passed its last read.
         if (s >= 3 && s + 3 < n3) {
             if (tid == 0) issue_plane(s + 3);
             issued = s + 4;
         }
+
+        // ---- finish p: x1 derivatives of F1, H21; P, H; store -----------------
+        if (valid && pin) {
+            const T *xf = xF1 + buf * NP + (pidx - i1 + s1);
+            const T *xh = xH21 + buf * NP + (pidx - i1 + s1);
+            T E1 = T(0), E21 = T(0);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                E1 += c1[k] * xf[k];
+                E21 += c1[k] * xh[k];
+            }
+            w1 += E1;
+            w2 += lpm * E21;
+            if (is_face) {
+                w1 = T(0.5) * (w1 + __shfl_xor_sync(facemask, w1, 1));
+                w2 = T(0.5) * (w2 + __shfl_xor_sync(facemask, w2, 1));
+            }
+            const bool ff = ff_x12 || p == 0 || p == n3 - 1;
+            const int rq = p < 4 ? p : (p >= n3 - 4 ? n3 - 1 - p : -1);
+            const T hw = ff ? T(0) : hpt * (rq >= 0 ? A3.wq[rq] : T(1));
+            const T y1 = hw * w1, y2 = hw * w2;
+            const long long o = ((long long)(side * 3 + 0) * n3 + p) * g.PS + ooff;
+            outcol[o] = (TO)y1;
+            outcol[o + (long long)n3 * g.PS] = (TO)y2;
+            const T va = v1w[CP], vb = v2w[CP];
+            if (MODE == MODE_RHS) {
+                acc0 += (double)y1 * (double)y1 + (double)y2 * (double)y2;
+            } else if (sizeof(T) == 4) {
+                acc0 += (double)(va * y1 + vb * y2);
+                acc1 += (double)(va * va + vb * vb);
+            } else {
+                acc0 += (double)va * (double)y1 + (double)vb * (double)y2;
+                acc1 += (double)va * (double)va + (double)vb * (double)vb;
+            }
+        }
+        // ---- finish z = s - 6: comp 3 --------------------------------------------
+        const int z = s - 6;
+        if (valid && z >= 0 && z < n3) {
+            T w3 = w3q[CZ] + x3_d1<CZ>(A3, F3w, z, n3);
+            if (is_face) w3 = T(0.5) * (w3 + __shfl_xor_sync(facemask, w3, 1));
+            const bool ff = ff_x12 || z == 0 || z == n3 - 1;
+            const int rq = z < 4 ? z : (z >= n3 - 4 ? n3 - 1 - z : -1);
+            const T hw = ff ? T(0) : hpt * (rq >= 0 ? A3.wq[rq] : T(1));
+            const T y3 = hw * w3;
+            const long long o = ((long long)(side * 3 + 2) * n3 + z) * g.PS + ooff;
+            outcol[o] = (TO)y3;
+            const T vc = v3w[CZ];
+            if (MODE == MODE_RHS) {
+                acc0 += (double)y3 * (double)y3;
+            } else if (sizeof(T) == 4) {
+                acc0 += (double)(vc * y3);
+                acc1 += (double)(vc * vc);
+            } else {
+                acc0 += (double)vc * (double)y3;
+                acc1 += (double)vc * (double)vc;
+            }
+        }
+        return true;
+    };
+
+    bool alive = true;
+    for (int s0 = 0; s0 < nsteps && alive; s0 += 7) {
+        alive = alive && (s0 + 0 >= nsteps || step(IC<0>{}, s0 + 0));
+        alive = alive && (s0 + 1 >= nsteps || step(IC<1>{}, s0 + 1));
+        alive = alive && (s0 + 2 >= nsteps || step(IC<2>{}, s0 + 2));
+        alive = alive && (s0 + 3 >= nsteps || step(IC<3>{}, s0 + 3));
+        alive = alive && (s0 + 4 >= nsteps || step(IC<4>{}, s0 + 4));
+        alive = alive && (s0 + 5 >= nsteps || step(IC<5>{}, s0 + 5));
+        alive = alive && (s0 + 6 >= nsteps || step(IC<6>{}, s0 + 6));
     }
 
-    if (dead) {
+    if (!alive) {
         // A wait gave up (recorded in *err). Before the CTA's shared memory is
         // released, wait (bounded) for every plane copy issued and not yet
         // consumed: planes dead_at .. issued-1.
         if (tid == 0) {
-            for (int q = dead_at; q < issued; ++q)
+            for (int q = max(dead_at, 0); q < issued; ++q)
                 mbar_wait_bounded(&mbar[q % EQD_NSLOT], (unsigned)((q / EQD_NSLOT) & 1), err);
         }
         __syncthreads();

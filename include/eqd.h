@@ -173,6 +173,13 @@ int eqd_stiffness_toeplitz(eqd_grid *grid, const eqd_solve_opts *opts, double *K
 int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t warmup, int32_t reps,
                       double *ms_per_launch, double *bytes_per_launch);
 
+/* Autotuner of the FP32 stencil launch configuration (x2 tile height, CTA
+ * size, CTAs per SM): times every variant on ncols device-resident columns,
+ * keeps the fastest for this grid (used by every later mixed-precision call)
+ * and reports the timings. Arrays hold *nvariants (<= 8) entries. */
+int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_per_variant, int32_t *tile_rows,
+                 int32_t *threads, int32_t *nvariants);
+
 /* Jacobi diagonal, `diag(A)` (src/ElasticitySplitNode.jl:352-357), reference layout. */
 int eqd_diag(eqd_grid *grid, double *d);
 
