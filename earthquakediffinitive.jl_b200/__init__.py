@@ -235,6 +235,19 @@ class FaultElasticity:
             pass
 
 
+def set_stencil_variant(fe, variant):
+    """Pin the FP32 stencil launch variant of this grid (skips autotuning)."""
+    check(lib().eqd_set_variant(fe.handle, C.c_int32(variant)))
+
+
+def autotune(fe, ncols=256):
+    """Time every FP32 stencil launch variant; returns (selected, [(tile_rows, threads, ms)])."""
+    sel, nv = C.c_int32(), C.c_int32()
+    ms, tr, tt = (C.c_double * 8)(), (C.c_int32 * 8)(), (C.c_int32 * 8)()
+    check(lib().eqd_autotune(fe.handle, C.c_int32(ncols), C.byref(sel), ms, tr, tt, C.byref(nv)))
+    return sel.value, [(tr[i], tt[i], ms[i]) for i in range(nv.value)]
+
+
 def frictional_node_count(fe):
     return fe.nf
 
@@ -274,12 +287,14 @@ def split_node_solve(solver, rhs):
 
 
 def apply_operator(fe, x, mode="A", precision="fp64"):
-    """y = A x (mode "A") or y = HP_DSAT x (mode "HP_DSAT"), reference layout."""
+    """y = A x (mode "A"), y = HP_DSAT x (mode "HP_DSAT"), or y = A x for x
+    already in range(P) (mode "A_rangeP", the kernel CG iterates with), in the
+    reference layout."""
     xx = f64(x)
     one = xx.ndim == 1
     X = np.ascontiguousarray((xx.reshape(-1, 1) if one else xx).T)
     Y = np.empty_like(X)
-    m = {"A": 0, "HP_DSAT": 1}[mode]
+    m = {"A": 0, "HP_DSAT": 1, "A_rangeP": 2}[mode]
     check(lib().eqd_apply(fe.handle, ptr(X), ptr(Y), C.c_int32(X.shape[0]), C.c_int32(m),
                           C.c_int32(_PRECISIONS[precision])))
     return Y[0].copy() if one else Y.T.copy()

@@ -357,7 +357,9 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
         for (int v = 0; v < kNumVariants; ++v) need = std::max(need, G->v32[v].smem);
         if ((size_t)optin < need)
             return fail(EQD_ERR_ARG, "stencil tile needs more shared memory than the device offers");
-        CUDA_OR_RETURN(configure_kernels((int)need));
+        // The limit is a per-kernel attribute shared by every grid of the
+        // process: set it to the device maximum, once per device.
+        CUDA_OR_RETURN(configure_kernels(optin));
     }
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
     CUDA_OR_RETURN(cudaEventCreate(&G->ev0));
@@ -424,6 +426,12 @@ static int apply_impl(eqd_grid *G, const double *x, double *y, int ncols, int mo
     cs.slip_comp = sc.as<int>();
     if (mode == 0) {
         CUDA_OR_RETURN((launch_march<T, T, MODE_AP>(G, dx.as<T>(), dy.as<T>(), cs, nullptr, ncols)));
+    } else if (mode == 2) {
+        DevBuf part;
+        int nt = G->m64.g.ntiles;
+        for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, G->v32[v].g.ntiles);
+        CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * nt));
+        CUDA_OR_RETURN((launch_march<T, T, MODE_A>(G, dx.as<T>(), dy.as<T>(), cs, part.as<double>(), ncols)));
     } else {
         CUDA_OR_RETURN((launch_march<T, T, MODE_RHS>(G, dx.as<T>(), dy.as<T>(), cs, nullptr, ncols)));
     }
@@ -438,7 +446,7 @@ static int apply_impl(eqd_grid *G, const double *x, double *y, int ncols, int mo
 extern "C" int eqd_apply(eqd_grid *G, const double *x, double *y, int32_t ncols, int32_t mode, int32_t precision) {
     if (!G || !x || !y) return fail(EQD_ERR_ARG, "null argument");
     if (ncols < 1) return fail(EQD_ERR_ARG, "ncols must be >= 1");
-    if (mode != 0 && mode != 1) return fail(EQD_ERR_ARG, "mode must be 0 (A) or 1 (HP_DSAT)");
+    if (mode < 0 || mode > 2) return fail(EQD_ERR_ARG, "mode must be 0 (A), 1 (HP_DSAT) or 2 (A, input in range(P))");
     std::lock_guard<std::mutex> lk(G->mtx);
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     if (precision == EQD_PREC_FP64) return apply_impl<double>(G, x, y, ncols, mode);
@@ -661,7 +669,11 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
         }
         CUDA_OR_RETURN(cudaMemsetAsync(W.iters.p, 0, sizeof(int) * chunk, G->stream));
         CUDA_OR_RETURN(cudaMemsetAsync(W.flag.p, 1, chunk, G->stream));
+        // Every vector starts at zero, padding included: the stencil's bulk
+        // copies bring plane padding into the rows beyond the x2 edge, which
+        // must read as zero, and the kernels never write the padding.
         CUDA_OR_RETURN(cudaMemsetAsync(W.x64.p, 0, sizeof(double) * vec, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(W.v0.p, 0, sizeof(T) * vec, G->stream));
         CUDA_OR_RETURN(cudaMemsetAsync(W.v1.p, 0, sizeof(T) * vec, G->stream));
         CUDA_OR_RETURN(cudaMemsetAsync(W.v2.p, 0, sizeof(T) * vec, G->stream));
         if (mixed) CUDA_OR_RETURN(cudaMemsetAsync(W.v3.p, 0, sizeof(float) * vec, G->stream));
@@ -683,7 +695,6 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
             cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), chunk, mixed);
         } else {
             // r0 = b given explicitly (reference layout, FP64).
-            CUDA_OR_RETURN(cudaMemsetAsync(W.v0.p, 0, sizeof(T) * vec, G->stream));
             CUDA_OR_RETURN(cudaMemcpyAsync(hbuf.p, B.rhs + (size_t)c0 * ntot, sizeof(double) * ntot * nc,
                                            cudaMemcpyHostToDevice, G->stream));
             const long long nel = ntot * nc;
@@ -992,6 +1003,14 @@ extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, doubl
         if (tile_rows) tile_rows[v] = G->v32[v].g.t2max;
         if (threads) threads[v] = G->v32[v].threads;
     }
+    return EQD_OK;
+}
+
+extern "C" int eqd_set_variant(eqd_grid *G, int32_t variant) {
+    if (!G || variant < 0 || variant >= kNumVariants) return fail(EQD_ERR_ARG, "invalid variant");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    G->sel32 = variant;
+    G->tuned = true;
     return EQD_OK;
 }
 

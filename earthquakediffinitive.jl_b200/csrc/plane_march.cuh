@@ -30,9 +30,8 @@
 //     x2-closure rows, fault nodes with the two sides in adjacent lanes);
 //   * x1 derivatives read the thread's own line from shared memory;
 //   * x2 derivatives read neighbouring rows (tile + 4-row halo) from shared;
-//   * x3 is marched plane by plane; x3 derivatives come from 7-slot register
-//     windows (closure rows reach +-3 planes), rotated by unrolling the march
-//     by 7 rather than by moving registers;
+//   * x3 is marched plane by plane; x3 derivatives come from 7-deep register
+//     windows (closure rows reach +-3 planes);
 //   * planes arrive through a 6-slot ring filled by cp.async.bulk copies
 //     completing on mbarriers, three planes ahead of use;
 //   * one CTA barrier per plane (the x1 exchange of F1/H21, double-buffered
@@ -84,95 +83,119 @@ struct MarchGeom {
     int i2f0, n2f, i3f0, n3f, nf;
 };
 
-// x3 derivatives from a 7-slot register window in which plane q lives in
-// slot q % 7; C0 is the (compile-time) slot of the centre plane q. Planes
-// outside the domain hold zero and meet zero coefficients.
-template <int C0, typename T>
+// x3 derivatives from a 7-deep register window ordered by age: w[6] is the
+// newest plane, the centre plane q sits in w[3]. Planes outside the domain
+// hold zero and meet zero coefficients.
+template <typename T>
 __device__ __forceinline__ T x3_d1(const AxisT<T> &a, const T (&w)[7], int q, int n3) {
     if (q >= 4 && q <= n3 - 5)
-        return a.d1_int[0] * w[(C0 + 5) % 7] + a.d1_int[1] * w[(C0 + 6) % 7] + a.d1_int[3] * w[(C0 + 1) % 7] +
-               a.d1_int[4] * w[(C0 + 2) % 7];
+        return a.d1_int[0] * w[1] + a.d1_int[1] * w[2] + a.d1_int[3] * w[4] + a.d1_int[4] * w[5];
     const int r = q < 4 ? q : 4 + (n3 - 1 - q);
     T s = T(0);
 #pragma unroll
-    for (int o = -3; o <= 3; ++o) s += a.d1_cl[r][o + 3] * w[(C0 + o + 7) % 7];
+    for (int o = 0; o < 7; ++o) s += a.d1_cl[r][o] * w[o];
     return s;
 }
 
-template <int C0, typename T>
+template <typename T>
 __device__ __forceinline__ T x3_d2(const AxisT<T> &a, const T (&w)[7], int q, int n3) {
     if (q >= 4 && q <= n3 - 5)
-        return a.d2_int[0] * w[(C0 + 5) % 7] + a.d2_int[1] * w[(C0 + 6) % 7] + a.d2_int[2] * w[C0] +
-               a.d2_int[3] * w[(C0 + 1) % 7] + a.d2_int[4] * w[(C0 + 2) % 7];
+        return a.d2_int[0] * w[1] + a.d2_int[1] * w[2] + a.d2_int[2] * w[3] + a.d2_int[3] * w[4] +
+               a.d2_int[4] * w[5];
     const int r = q < 4 ? q : 4 + (n3 - 1 - q);
     T s = T(0);
 #pragma unroll
-    for (int o = -3; o <= 3; ++o) s += a.d2_cl[r][o + 3] * w[(C0 + o + 7) % 7];
-    return s;
-}
-
-// x2-direction D1 / D2 / W at row r of a chunk pointer `c` (own element),
-// row stride n1: the interior stencil everywhere (rows beyond the domain read
-// zeros) plus, for closure rows (`cl`), the closure correction.
-template <typename T>
-__device__ __forceinline__ T x2_d1(const AxisT<T> &a, const T *c, int n1, int r, int n2, bool cl) {
-    T s = a.d1_int[0] * c[-2 * n1] + a.d1_int[1] * c[-n1] + a.d1_int[3] * c[n1] + a.d1_int[4] * c[2 * n1];
-    if (cl) {
-        if (r < 4) {
-            const T *b = c - r * n1;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) s += a.d1_corrL[r][k] * b[k * n1];
-        } else if (r >= n2 - 4) {
-            const int rr = n2 - 1 - r;
-            const T *b = c + rr * n1;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) s += a.d1_corrR[rr][k] * b[-k * n1];
-        }
-    }
+    for (int o = 0; o < 7; ++o) s += a.d2_cl[r][o] * w[o];
     return s;
 }
 
 template <typename T>
-__device__ __forceinline__ T x2_d2(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2, bool cl) {
-    T s = a.d2_int[0] * c[-2 * n1] + a.d2_int[1] * c[-n1] + a.d2_int[2] * self + a.d2_int[3] * c[n1] +
-          a.d2_int[4] * c[2 * n1];
-    if (cl) {
-        if (r < 4) {
-            const T *b = c - r * n1;
+__device__ __forceinline__ void push7(T (&w)[7], T v) {
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += a.d2_corrL[r][k] * b[k * n1];
-        } else if (r >= n2 - 4) {
-            const int rr = n2 - 1 - r;
-            const T *b = c + rr * n1;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) s += a.d2_corrR[rr][k] * b[-k * n1];
-        }
-    }
-    return s;
+    for (int k = 0; k < 6; ++k) w[k] = w[k + 1];
+    w[6] = v;
+}
+
+// x2-direction operators at row r of a chunk pointer `c` (own element), row
+// stride n1. The interior stencils are applied everywhere (rows beyond the
+// domain read zero); threads on closure rows (`cl`) then add the closure
+// corrections, one pass over the rows per input.
+template <typename T>
+__device__ __forceinline__ T x2_d1i(const AxisT<T> &a, const T *c, int n1) {
+    return a.d1_int[0] * c[-2 * n1] + a.d1_int[1] * c[-n1] + a.d1_int[3] * c[n1] + a.d1_int[4] * c[2 * n1];
 }
 
 template <typename T>
-__device__ __forceinline__ T x2_w(const AxisT<T> &a, const T *c, T self, int n1, int r, int n2, bool cl) {
+__device__ __forceinline__ T x2_d2i(const AxisT<T> &a, const T *c, T self, int n1) {
+    return a.d2_int[0] * c[-2 * n1] + a.d2_int[1] * c[-n1] + a.d2_int[2] * self + a.d2_int[3] * c[n1] +
+           a.d2_int[4] * c[2 * n1];
+}
+
+template <typename T>
+__device__ __forceinline__ T x2_wi(const AxisT<T> &a, const T *c, T self, int n1) {
     T s = a.w_int[4] * self;
 #pragma unroll
     for (int o = 1; o <= 4; ++o) s += a.w_int[4 - o] * c[-o * n1] + a.w_int[4 + o] * c[o * n1];
-    if (cl) {
-        if (r < 6) {
-            const T *b = c - r * n1;
-#pragma unroll
-            for (int k = 0; k < 11; ++k) s += a.w_corrL[r][k] * b[k * n1];
-        } else if (r >= n2 - 6) {
-            const int rr = n2 - 1 - r;
-            const T *b = c + rr * n1;
-#pragma unroll
-            for (int k = 0; k < 11; ++k) s += a.w_corrR[rr][k] * b[-k * n1];
-        }
-    }
     return s;
 }
 
-template <int V>
-using IC = std::integral_constant<int, V>;
+// Closure correction geometry of row r for an operator whose closure rows
+// are the first / last `ncl` rows: whether row r is a closure row, its first
+// boundary row (offset from the own element), the stride toward the
+// interior, and the table row. For short axes where both closures reach a
+// row, the lower-end table (built from the exact matrix) covers the whole row.
+struct X2Corr {
+    int off;
+    int step;
+    int row;
+    bool left;
+    bool on;
+};
+
+__device__ __forceinline__ X2Corr x2_geom(int r, int n1, int n2, int ncl) {
+    X2Corr g;
+    g.left = r < ncl;
+    g.on = g.left || r >= n2 - ncl;
+    g.row = g.left ? r : n2 - 1 - r;
+    g.off = g.left ? -r * n1 : g.row * n1;
+    g.step = g.left ? n1 : -n1;
+    return g;
+}
+
+// D1 and D2 corrections on one input (closure rows 0..3 / n-4..n-1, 6 columns).
+template <typename T>
+__device__ __forceinline__ void x2_corr_dd(const AxisT<T> &a, const X2Corr &q, const T *c, T &d1, T &d2) {
+    if (!q.on) return;
+    const T *t1 = q.left ? a.d1_corrL[q.row] : a.d1_corrR[q.row];
+    const T *t2 = q.left ? a.d2_corrL[q.row] : a.d2_corrR[q.row];
+    const T *b = c + q.off;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const T x = b[k * q.step];
+        d1 += t1[k] * x;
+        d2 += t2[k] * x;
+    }
+}
+
+// D1-only correction (for H23 at ingest).
+template <typename T>
+__device__ __forceinline__ void x2_corr_d1(const AxisT<T> &a, const X2Corr &q, const T *c, T &d1) {
+    if (!q.on) return;
+    const T *t1 = q.left ? a.d1_corrL[q.row] : a.d1_corrR[q.row];
+    const T *b = c + q.off;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) d1 += t1[k] * b[k * q.step];
+}
+
+// W correction (closure rows 0..5 / n-6..n-1, 11 columns).
+template <typename T>
+__device__ __forceinline__ void x2_corr_w(const AxisT<T> &a, const X2Corr &q, const T *c, T &w) {
+    if (!q.on) return;
+    const T *tw = q.left ? a.w_corrL[q.row] : a.w_corrR[q.row];
+    const T *b = c + q.off;
+#pragma unroll
+    for (int k = 0; k < 11; ++k) w += tw[k] * b[k * q.step];
+}
 
 template <typename T, typename TO, int MODE, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
@@ -245,6 +268,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const bool valid = cls < 3;
     const bool is_face = cls == 2;
     const bool x2cl = cls != 0 && (i2 < 6 || i2 >= n2 - 6);
+    const X2Corr gdd = x2_geom(i2, n1, n2, 4);
+    const X2Corr gw = x2_geom(i2, n1, n2, 6);
     const unsigned facemask = __ballot_sync(0xffffffffu, is_face);
     const int i2l = i2 - a0;
     const int pidx = (side * g.t2max + i2l) * n1 + i1;
@@ -331,12 +356,9 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const int nsteps = n3 + 6;
     int dead_at = -1;
 
-    // One march step. Plane q of every window lives in slot q % 7; the step
-    // index modulo 7 is a compile-time constant R.
-    auto step = [&](auto Rc, int s) -> bool {
-        constexpr int R = decltype(Rc)::value;
-        constexpr int CP = (R + 4) % 7;  // slot of p = s - 3
-        constexpr int CZ = (R + 1) % 7;  // slot of z = s - 6
+    // One march step. Windows are ordered by age: index 6 holds plane s,
+    // index 3 plane p = s - 3; the F3 and w3 queues hold p at 6, z = s - 6 at 3.
+    auto step = [&](int s) -> bool {
         const int buf = s & 1;
         // ---- ingest plane s ----------------------------------------------------
         if (s < n3) {
@@ -388,18 +410,25 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 fence_proxy_async_smem();
                 __syncthreads();
             }
+            T a = T(0), b = T(0), c = T(0), h = T(0);
             if (valid) {
                 const T *pl = ring + (size_t)slot * 6 * g.CH;
                 const T *c3 = pl + (side * 3 + 2) * g.CH + own;
-                v1w[R] = pl[(side * 3 + 0) * g.CH + own];
-                v2w[R] = pl[(side * 3 + 1) * g.CH + own];
-                v3w[R] = c3[0];
-                H23w[R] = x2_d1(A2, c3, n1, i2, n2, x2cl);
-            } else {
-                v1w[R] = v2w[R] = v3w[R] = H23w[R] = T(0);
+                a = pl[(side * 3 + 0) * g.CH + own];
+                b = pl[(side * 3 + 1) * g.CH + own];
+                c = c3[0];
+                h = x2_d1i(A2, c3, n1);
+                if (x2cl) x2_corr_d1(A2, gdd, c3, h);
             }
+            push7(v1w, a);
+            push7(v2w, b);
+            push7(v3w, c);
+            push7(H23w, h);
         } else {
-            v1w[R] = v2w[R] = v3w[R] = H23w[R] = T(0);
+            push7(v1w, T(0));
+            push7(v2w, T(0));
+            push7(v3w, T(0));
+            push7(H23w, T(0));
         }
 
         // ---- in-plane work at p = s - 3 ---------------------------------------
@@ -414,7 +443,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             const T *o1 = pl + (side * 3 + 0) * g.CH + own;
             const T *o2 = pl + (side * 3 + 1) * g.CH + own;
             const T *o3 = pl + (side * 3 + 2) * g.CH + own;
-            const T v1 = v1w[CP], v2 = v2w[CP], v3 = v3w[CP];
+            const T v1 = v1w[3], v2 = v2w[3], v3 = v3w[3];
             T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
@@ -424,17 +453,24 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 A21 += c2[k] * x2;
                 A31 += c2[k] * x3;
             }
-            const T G2 = x2_d1(A2, o2, n1, i2, n2, x2cl);
-            const T H21 = x2_d1(A2, o1, n1, i2, n2, x2cl);
-            const T A12 = x2_d2(A2, o1, v1, n1, i2, n2, x2cl);
-            const T A22 = x2_d2(A2, o2, v2, n1, i2, n2, x2cl);
-            const T A32 = x2_d2(A2, o3, v3, n1, i2, n2, x2cl);
-            const T W2 = x2_w(A2, o2, v2, n1, i2, n2, x2cl);
-            const T G3 = x3_d1<CP>(A3, v3w, p, n3);
-            const T A13 = x3_d2<CP>(A3, v1w, p, n3);
-            const T A23 = x3_d2<CP>(A3, v2w, p, n3);
-            const T A33 = x3_d2<CP>(A3, v3w, p, n3);
-            const T D3H23 = x3_d1<CP>(A3, H23w, p, n3);
+            T G2 = x2_d1i(A2, o2, n1);
+            T H21 = x2_d1i(A2, o1, n1);
+            T A12 = x2_d2i(A2, o1, v1, n1);
+            T A22 = x2_d2i(A2, o2, v2, n1);
+            T A32 = x2_d2i(A2, o3, v3, n1);
+            T W2 = x2_wi(A2, o2, v2, n1);
+            if (x2cl) {
+                T dummy = T(0);
+                x2_corr_dd(A2, gdd, o1, H21, A12);
+                x2_corr_dd(A2, gdd, o2, G2, A22);
+                x2_corr_dd(A2, gdd, o3, dummy, A32);
+                x2_corr_w(A2, gw, o2, W2);
+            }
+            const T G3 = x3_d1(A3, v3w, p, n3);
+            const T A13 = x3_d2(A3, v1w, p, n3);
+            const T A23 = x3_d2(A3, v2w, p, n3);
+            const T A33 = x3_d2(A3, v3w, p, n3);
+            const T D3H23 = x3_d1(A3, H23w, p, n3);
             const T F1 = lam * G1 + lpm * (G2 + G3);
             F3 = lam * G3 + lpm * (G1 + G2);
             w1 = mu * (T(2) * A11 + A12 + A13);
@@ -455,7 +491,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                     dh2 += cf * l2[q];
                     dh3 += cf * l3[q];
                 }
-                const T D3v1 = x3_d1<CP>(A3, v1w, p, n3);
+                const T D3v1 = x3_d1(A3, v1w, p, n3);
                 const T tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
                 const T tau2 = mu * (H21 + dh2);
                 const T tau3 = mu * (D3v1 + dh3);
@@ -470,8 +506,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             xF1[buf * NP + pidx] = F1;
             xH21[buf * NP + pidx] = H21;
         }
-        F3w[CP] = F3;
-        w3q[CP] = w3p;
+        push7(F3w, F3);
+        push7(w3q, w3p);
         __syncthreads();
         if (s_dead[buf]) {
             dead_at = s;
@@ -506,7 +542,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             const long long o = ((long long)(side * 3 + 0) * n3 + p) * g.PS + ooff;
             outcol[o] = (TO)y1;
             outcol[o + (long long)n3 * g.PS] = (TO)y2;
-            const T va = v1w[CP], vb = v2w[CP];
+            const T va = v1w[3], vb = v2w[3];
             if (MODE == MODE_RHS) {
                 acc0 += (double)y1 * (double)y1 + (double)y2 * (double)y2;
             } else if (sizeof(T) == 4) {
@@ -520,7 +556,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         // ---- finish z = s - 6: comp 3 --------------------------------------------
         const int z = s - 6;
         if (valid && z >= 0 && z < n3) {
-            T w3 = w3q[CZ] + x3_d1<CZ>(A3, F3w, z, n3);
+            T w3 = w3q[3] + x3_d1(A3, F3w, z, n3);
             if (is_face) w3 = T(0.5) * (w3 + __shfl_xor_sync(facemask, w3, 1));
             const bool ff = ff_x12 || z == 0 || z == n3 - 1;
             const int rq = z < 4 ? z : (z >= n3 - 4 ? n3 - 1 - z : -1);
@@ -528,7 +564,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             const T y3 = hw * w3;
             const long long o = ((long long)(side * 3 + 2) * n3 + z) * g.PS + ooff;
             outcol[o] = (TO)y3;
-            const T vc = v3w[CZ];
+            const T vc = v3w[0];
             if (MODE == MODE_RHS) {
                 acc0 += (double)y3 * (double)y3;
             } else if (sizeof(T) == 4) {
@@ -543,15 +579,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     };
 
     bool alive = true;
-    for (int s0 = 0; s0 < nsteps && alive; s0 += 7) {
-        alive = alive && (s0 + 0 >= nsteps || step(IC<0>{}, s0 + 0));
-        alive = alive && (s0 + 1 >= nsteps || step(IC<1>{}, s0 + 1));
-        alive = alive && (s0 + 2 >= nsteps || step(IC<2>{}, s0 + 2));
-        alive = alive && (s0 + 3 >= nsteps || step(IC<3>{}, s0 + 3));
-        alive = alive && (s0 + 4 >= nsteps || step(IC<4>{}, s0 + 4));
-        alive = alive && (s0 + 5 >= nsteps || step(IC<5>{}, s0 + 5));
-        alive = alive && (s0 + 6 >= nsteps || step(IC<6>{}, s0 + 6));
-    }
+    for (int s = 0; s < nsteps && alive; ++s) alive = step(s);
 
     if (!alive) {
         // A wait gave up (recorded in *err). Before the CTA's shared memory is

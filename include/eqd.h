@@ -131,6 +131,8 @@ int eqd_grid_fault_axes(const eqd_grid *grid, double *x2f, double *x3f);
  * mode 0: y = A x          (A = -H P (D+SAT) P; `mul!(y, A, x)` on the
  *                            assembled matrix of src/ElasticitySplitNode.jl:211)
  * mode 1: y = HP_DSAT x    (= H P (D+SAT) x, the RHS operator of :210)
+ * mode 2: y = A x for x already in range(P) (the kernel the CG iterations
+ *         run; skips the input projection)
  * precision: EQD_PREC_FP64 or EQD_PREC_MIXED (FP32 arithmetic). */
 int eqd_apply(eqd_grid *grid, const double *x, double *y, int32_t ncols, int32_t mode, int32_t precision);
 
@@ -179,6 +181,10 @@ int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t 
  * and reports the timings. Arrays hold *nvariants (<= 8) entries. */
 int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_per_variant, int32_t *tile_rows,
                  int32_t *threads, int32_t *nvariants);
+
+/* Pins the FP32 stencil launch variant (0 .. *nvariants-1 of eqd_autotune)
+ * for this grid instead of autotuning (reproducibility across processes). */
+int eqd_set_variant(eqd_grid *grid, int32_t variant);
 
 /* Jacobi diagonal, `diag(A)` (src/ElasticitySplitNode.jl:352-357), reference layout. */
 int eqd_diag(eqd_grid *grid, double *d);

@@ -67,3 +67,20 @@ def test_apply_columns_independent(eqd):
         Y = eqd.apply_operator(fe, X, mode="A", precision=precision)
         y2 = eqd.apply_operator(fe, X[:, 2], mode="A", precision=precision)
         assert np.array_equal(Y[:, 2], y2)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}")
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_cg_path_kernel_every_variant(eqd, case, variant):
+    """The kernel the CG iterations run (input already in range(P)), for each
+    FP32 launch variant the autotuner may pick, and in FP64."""
+    S = oracle_system(case)
+    fe = gpu_fe(eqd, case)
+    eqd.set_stencil_variant(fe, variant)
+    X = S.P @ np.random.default_rng(5).standard_normal((S.Ntot, 2))
+    for precision, tol in (("mixed", 2e-5), ("fp64", 1e-12)):
+        Y = eqd.apply_operator(fe, X, mode="A_rangeP", precision=precision)
+        for j in range(X.shape[1]):
+            ref = S.A @ X[:, j]
+            err = abs(Y[:, j] - ref).max() / abs(S.A).dot(abs(X[:, j])).max()
+            assert err < tol, (precision, j, err)
