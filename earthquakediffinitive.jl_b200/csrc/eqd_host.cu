@@ -1079,3 +1079,68 @@ extern "C" int eqd_kmat_destroy(eqd_kmat *M) {
     delete M;
     return EQD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free GEMV.
+//
+// For callers that must not allocate device memory at all: a time loop that
+// runs inside a CUDA graph or under a framework's own device allocator (a
+// Julia CuArray pool, a PyTorch caching allocator), where a hidden cudaMalloc
+// would break capture or fragment the caller's pool, and latency-critical
+// loops that may not block on the allocator. The caller passes K, s and y as
+// device pointers it already owns; the only scratch (the per-slice partial
+// row sums of the two-pass GEMV) lives in this file-scope array, 4 MiB per
+// device, held by every GPU that loads the library until exit. The first call
+// on a device looks the array's device address up (with that device current);
+// make that first call before any stream capture. All calls on a device share
+// the array: calls that overlap on the GPU race, so serialise them (one
+// stream, or events). The array keeps the last call's contents; nothing in it
+// needs to start at zero, because every partial sum read in a call was written
+// in the same call.
+// ---------------------------------------------------------------------------
+#define EQD_GEMV_STATIC_SCRATCH_DOUBLES (1 << 19)
+
+static __device__ __align__(256) double g_gemv_static_scratch[EQD_GEMV_STATIC_SCRATCH_DOUBLES];
+
+static std::mutex g_gemv_static_mtx;
+static double *g_gemv_static_ptr[128] = {nullptr};
+
+extern "C" int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_device, const double *s_device,
+                                    double *y_device, int32_t nvec, void *stream) {
+    if (n < 1 || nvec < 1 || !K_device || !s_device || !y_device) return fail(EQD_ERR_ARG, "invalid argument");
+    if ((long long)n * nvec > EQD_GEMV_STATIC_SCRATCH_DOUBLES)
+        return fail(EQD_ERR_ARG, "eqd_kmat_gemv_static: n * nvec = " + std::to_string((long long)n * nvec) +
+                                     " exceeds the static scratch of " +
+                                     std::to_string(EQD_GEMV_STATIC_SCRATCH_DOUBLES) + " doubles");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev || device >= 128) return fail(EQD_ERR_ARG, "device ordinal out of range");
+    int prev = 0;
+    CUDA_OR_RETURN(cudaGetDevice(&prev));
+    if (prev != device) CUDA_OR_RETURN(cudaSetDevice(device));
+    double *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_gemv_static_mtx);
+        if (!g_gemv_static_ptr[device]) {
+            void *ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_gemv_static_scratch);
+            if (e != cudaSuccess) {
+                if (prev != device) cudaSetDevice(prev);
+                return fail(EQD_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            }
+            g_gemv_static_ptr[device] = static_cast<double *>(ptr);
+        }
+        scratch = g_gemv_static_ptr[device];
+    }
+    int nslice = gemv_slices(n);
+    nslice = std::max(1, std::min<int>(nslice, (int)(EQD_GEMV_STATIC_SCRATCH_DOUBLES / ((long long)n * nvec))));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
+    gemv_partial_kernel<<<grid, 256, 0, st>>>(K_device, s_device, n, nslice, nvec, scratch);
+    const long long ne = (long long)n * nvec;
+    gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(scratch, n, nslice, nvec, y_device);
+    cudaError_t e = cudaGetLastError();
+    if (prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("eqd_kmat_gemv_static launch: ") + cudaGetErrorString(e));
+    return EQD_OK;
+}

@@ -195,6 +195,18 @@ int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out);
 int eqd_kmat_gemv(eqd_kmat *kmat, const double *s, double *y, int32_t nvec);
 int eqd_kmat_destroy(eqd_kmat *kmat);
 
+/* Allocation-free y = K s (no counterpart in the reference: an addition for
+ * callers that cannot allocate device memory, e.g. a time loop inside CUDA
+ * graph capture or under a framework's own allocator). K (n x n, column-major),
+ * s and y (n x nvec) are DEVICE pointers owned by the caller, on `device`.
+ * Scratch is a static 4 MiB array per device: n * nvec must not exceed
+ * 524,288 (EQD_ERR_ARG otherwise). The first call on a device looks the array
+ * up (make it before any stream capture). Launches on `stream` (a
+ * cudaStream_t, NULL = default stream) and returns without synchronizing;
+ * calls that overlap on the GPU share the scratch and race. */
+int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_device, const double *s_device,
+                         double *y_device, int32_t nvec, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
