@@ -122,7 +122,7 @@ class CGSolver:
     FP64 true residual."""
 
     def __init__(self, fe=None, rtol=1e-10, atol=0.0, itmax=0, precond="none", precision="mixed",
-                 chunk=0, reliable_delta=0.1, hbm_budget_bytes=0, tile_rows=0):
+                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0):
         if precond not in _PRECONDS:
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precond must be :none or :jacobi, got {precond}")
         if precision not in _PRECISIONS:

@@ -69,12 +69,19 @@ struct MarchCfg {
 
 static constexpr int kMaxT32 = 640;   // generic FP32 instances
 static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register spills
+static constexpr int kMaxT32c = 384;  // FP32 A-apply, two columns per thread
 static constexpr int kMaxT64 = 384;
-static constexpr int kNumVariants = 3;
+static constexpr int kNumVariants = 5;
 
+static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
+
+// `maxt` limits the threads of the tile; `kmaxt` is the launch bound of the
+// kernel instance that will run it (it fixes the shared-memory geometry of
+// the n1-specialized instances).
 template <typename T>
 static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, int maxt, int tile_rows,
-                           const GridConst &gc, MarchCfg &out, std::string &why) {
+                           const GridConst &gc, MarchCfg &out, std::string &why, int lanes = 1, int kmaxt = 0) {
+    if (kmaxt == 0) kmaxt = maxt;
     const int per_row = 2 * n1;
     int t2 = tile_rows > 0 ? std::min(tile_rows, maxt / per_row) : maxt / per_row;
     t2 = std::min(t2, n2);
@@ -92,6 +99,15 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     constexpr int AE = 16 / (int)sizeof(T);
     int CH = (t2max + 2 * EQD_HALO) * n1 + 2 * AE;
     CH = (CH + AE - 1) / AE * AE;
+    int NP = 2 * n1 * t2max;
+    if (n1_specialized(n1)) {
+        if (t2max > march_t2cap(n1, kmaxt)) {
+            why = "tile exceeds the specialized kernel's capacity";
+            return false;
+        }
+        CH = march_chcap(n1, kmaxt, (int)sizeof(T));
+        NP = 2 * n1 * march_t2cap(n1, kmaxt);
+    }
     out.g.n1 = n1;
     out.g.n2 = n2;
     out.g.n3 = n3;
@@ -108,8 +124,9 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     int threads = per_row * t2max;
     threads = (threads + 31) / 32 * 32;
     out.threads = threads;
-    // barriers + flags, reduction scratch, plane ring, F1/H21 exchange [2][points] x 2
-    out.smem = 64 + 32 * 8 + (size_t)EQD_NSLOT * 6 * CH * sizeof(T) + 4 * (size_t)(2 * n1 * t2max) * sizeof(T);
+    // barriers + flags, reduction scratch, and per column: plane ring, F1/H21
+    // exchange [2][points] x 2
+    out.smem = 64 + 32 * 8 + (size_t)lanes * ((size_t)EQD_NSLOT * 6 * CH + 4 * (size_t)NP) * sizeof(T);
     return true;
 }
 
@@ -151,10 +168,11 @@ struct eqd_grid {
     MarchCfg m32, m64;
     // FP32 A-apply launch variants (see make_variants) and the chosen one.
     MarchCfg v32[kNumVariants];
-    int v32_maxt[kNumVariants] = {0, 0, 0};
+    int v32_maxt[kNumVariants] = {};
+    int v32_lanes[kNumVariants] = {};
     int sel32 = 0;
     bool tuned = false;
-    double tune_ms[kNumVariants] = {0, 0, 0};
+    double tune_ms[kNumVariants] = {};
     int nchunks = 1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -175,47 +193,80 @@ struct eqd_kmat {
 // ---------------------------------------------------------------------------
 // Kernel launch helpers
 // ---------------------------------------------------------------------------
+// Kernel instances compiled for a fixed n1 (the BP8 grids' 9, 21, 33 points
+// across a side); any other n1 runs the runtime-n1 instance.
+#define EQD_FOR_N1(X) X(9) X(21) X(33)
+
+template <typename T, typename TO, int MODE, int MAXT, int L = 1>
+static void launch_n1(int n1, dim3 grid, const MarchCfg &m, cudaStream_t st, const OpConst<T> &C, const T *in,
+                      TO *out, ColumnSet cs, double *partials, unsigned *err) {
+    switch (n1) {
+#define EQD_CASE(N)                                                                                       \
+    case N:                                                                                               \
+        plane_march_kernel<T, TO, MODE, MAXT, N, L><<<grid, m.threads, m.smem, st>>>(C, m.g, in, out, cs, \
+                                                                                     partials, err);      \
+        return;
+        EQD_FOR_N1(EQD_CASE)
+#undef EQD_CASE
+    default:
+        plane_march_kernel<T, TO, MODE, MAXT, 0, L><<<grid, m.threads, m.smem, st>>>(C, m.g, in, out, cs,
+                                                                                     partials, err);
+    }
+}
+
 template <typename T, typename TO, int MODE>
 static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols,
                                 int variant = -1) {
+    cs.ncols = ncols;
+    const int n1 = G->gc.n1;
     if (sizeof(T) == 4 && MODE == MODE_A) {
         const int v = variant >= 0 ? variant : G->sel32;
         const MarchCfg &m = G->v32[v];
-        cs.ncols = ncols;
-        dim3 grid((unsigned)(ncols * m.g.ntiles));
+        const int lanes = G->v32_lanes[v];
+        dim3 grid((unsigned)(((ncols + lanes - 1) / lanes) * m.g.ntiles));
         const float *fin = reinterpret_cast<const float *>(in);
         float *fout = reinterpret_cast<float *>(out);
-        if (G->v32_maxt[v] == kMaxT32)
-            plane_march_kernel<float, float, MODE_A, kMaxT32><<<grid, m.threads, m.smem, G->stream>>>(
-                G->c32, m.g, fin, fout, cs, partials, G->err.as<unsigned>());
+        if (lanes == 2)
+            launch_n1<float, float, MODE_A, kMaxT32c, 2>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+                                                          G->err.as<unsigned>());
+        else if (G->v32_maxt[v] == kMaxT32)
+            launch_n1<float, float, MODE_A, kMaxT32>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+                                                     G->err.as<unsigned>());
         else
-            plane_march_kernel<float, float, MODE_A, kMaxT32b><<<grid, m.threads, m.smem, G->stream>>>(
-                G->c32, m.g, fin, fout, cs, partials, G->err.as<unsigned>());
+            launch_n1<float, float, MODE_A, kMaxT32b>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+                                                      G->err.as<unsigned>());
         return cudaGetLastError();
     }
     constexpr int MAXT = sizeof(T) == 4 ? kMaxT32 : kMaxT64;
     const MarchCfg &m = sizeof(T) == 4 ? G->m32 : G->m64;
     const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
                                                                                : (const void *)&G->c64);
-    auto kern = plane_march_kernel<T, TO, MODE, MAXT>;
-    cs.ncols = ncols;
     dim3 grid((unsigned)(ncols * m.g.ntiles));
-    kern<<<grid, m.threads, m.smem, G->stream>>>(C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+    if (MODE == MODE_AP) {  // generic-input hook: runtime-n1 instance only
+        plane_march_kernel<T, TO, MODE, MAXT, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
+            C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+    } else {
+        launch_n1<T, TO, MODE, MAXT>(n1, grid, m, G->stream, C, in, out, cs, partials, G->err.as<unsigned>());
+    }
     return cudaGetLastError();
 }
 
 // Dynamic shared memory above 48 KB must be opted into per kernel.
 static cudaError_t configure_kernels(int smem_max) {
+#define EQD_KS(N)                                                                \
+    (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32, N, 1>,       \
+        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32b, N, 1>,    \
+        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32c, N, 2>,    \
+        (const void *)plane_march_kernel<float, float, MODE_RHS, kMaxT32, N, 1>,   \
+        (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64, N, 1>,   \
+        (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64, N, 1>, \
+        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64, N, 1>,
     const void *ks[] = {
-        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32>,
-        (const void *)plane_march_kernel<float, float, MODE_A, kMaxT32b>,
-        (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32>,
-        (const void *)plane_march_kernel<float, float, MODE_RHS, kMaxT32>,
-        (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64>,
-        (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64>,
-        (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64>,
-        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64>,
+        EQD_FOR_N1(EQD_KS) EQD_KS(0)
+        (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32, 0, 1>,
+        (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64, 0, 1>,
     };
+#undef EQD_KS
     for (const void *k : ks) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
         if (e != cudaSuccess) return e;
@@ -249,7 +300,7 @@ extern "C" void eqd_default_opts(eqd_solve_opts *o) {
     o->precond = EQD_PRECOND_NONE;
     o->precision = EQD_PREC_MIXED;
     o->chunk = 0;
-    o->reliable_delta = 0.1;
+    o->reliable_delta = 0.01;
     o->hbm_budget_bytes = 0;
     o->tile_rows = 0;
     o->flags = 0;
@@ -336,13 +387,18 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     // spill), one CTA of up to 512 threads (no spill), and CTAs of up to 256
     // threads so that two share an SM.
     {
-        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256};
-        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b};
+        // thread limit, kernel launch bound, columns per thread
+        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192};
+        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c};
+        const int ln[kNumVariants] = {1, 1, 1, 2, 2};
         for (int v = 0; v < kNumVariants; ++v) {
             G->v32_maxt[v] = mt[v];
-            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], 0, gc, G->v32[v], why)) {
+            G->v32_lanes[v] = ln[v];
+            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], 0, gc, G->v32[v], why,
+                                       ln[v], mt[v])) {
                 G->v32[v] = G->m32;  // fall back to the generic configuration
                 G->v32_maxt[v] = kMaxT32;
+                G->v32_lanes[v] = 1;
             }
         }
         G->sel32 = 1;
@@ -618,7 +674,7 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
     sp.rtol = o.rtol;
     sp.atol = o.atol;
     sp.itmax = o.itmax;
-    sp.delta = o.reliable_delta > 0 ? o.reliable_delta : 0.1;
+    sp.delta = o.reliable_delta > 0 ? o.reliable_delta : 0.01;
     sp.ntiles = ntA;
     sp.nchunks = G->nchunks;
     sp.colstride = gc.colstride;

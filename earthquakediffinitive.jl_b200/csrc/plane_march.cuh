@@ -74,6 +74,15 @@ struct OpConst {
     double hvol;
 };
 
+// Shared-memory geometry of a kernel compiled for a fixed n1 (N1 > 0): the
+// chunk capacity and the exchange-array size are those of the largest tile
+// the launch bound admits, so every offset is a compile-time constant.
+__host__ __device__ constexpr int march_t2cap(int n1, int maxt) { return maxt / (2 * n1); }
+__host__ __device__ constexpr int march_chcap(int n1, int maxt, int elem_bytes) {
+    return (((march_t2cap(n1, maxt) + 2 * EQD_HALO) * n1 + 2 * (16 / elem_bytes)) + (16 / elem_bytes) - 1) /
+           (16 / elem_bytes) * (16 / elem_bytes);
+}
+
 struct MarchGeom {
     int n1, n2, n3, PS;
     long long colstride;
@@ -86,6 +95,30 @@ struct MarchGeom {
 // x3 derivatives from a 7-deep register window ordered by age: w[6] is the
 // newest plane, the centre plane q sits in w[3]. Planes outside the domain
 // hold zero and meet zero coefficients.
+template <typename T>
+__device__ __forceinline__ T x3_d1i(const AxisT<T> &a, const T (&w)[7]) {
+    return a.d1_int[0] * w[1] + a.d1_int[1] * w[2] + a.d1_int[3] * w[4] + a.d1_int[4] * w[5];
+}
+template <typename T>
+__device__ __forceinline__ T x3_d2i(const AxisT<T> &a, const T (&w)[7]) {
+    return a.d2_int[0] * w[1] + a.d2_int[1] * w[2] + a.d2_int[2] * w[3] + a.d2_int[3] * w[4] + a.d2_int[4] * w[5];
+}
+// Closure row r (0..3 lower end, 4..7 upper end) of the x3 operators.
+template <typename T>
+__device__ __forceinline__ T x3_d1c(const AxisT<T> &a, const T (&w)[7], int r) {
+    T s = T(0);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) s += a.d1_cl[r][o] * w[o];
+    return s;
+}
+template <typename T>
+__device__ __forceinline__ T x3_d2c(const AxisT<T> &a, const T (&w)[7], int r) {
+    T s = T(0);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) s += a.d2_cl[r][o] * w[o];
+    return s;
+}
+
 template <typename T>
 __device__ __forceinline__ T x3_d1(const AxisT<T> &a, const T (&w)[7], int q, int n3) {
     if (q >= 4 && q <= n3 - 5)
@@ -107,6 +140,16 @@ __device__ __forceinline__ T x3_d2(const AxisT<T> &a, const T (&w)[7], int q, in
 #pragma unroll
     for (int o = 0; o < 7; ++o) s += a.d2_cl[r][o] * w[o];
     return s;
+}
+
+// Quadrature weight H3/h3 of x3-plane q, zero on the far-field planes
+// (q = 0, n3-1) and outside the domain.
+template <typename T>
+__device__ __forceinline__ T plane_weight(const AxisT<T> &a, int q, int n3) {
+    if (q <= 0 || q >= n3 - 1) return T(0);
+    if (q < 4) return a.wq[q];
+    if (q >= n3 - 4) return a.wq[n3 - 1 - q];
+    return T(1);
 }
 
 template <typename T>
@@ -197,18 +240,41 @@ __device__ __forceinline__ void x2_corr_w(const AxisT<T> &a, const X2Corr &q, co
     for (int k = 0; k < 11; ++k) w += tw[k] * b[k * q.step];
 }
 
-template <typename T, typename TO, int MODE, int MAXT>
+// N1 > 0 compiles the kernel for that fixed number of x1 points per side
+// (every shared-memory offset becomes an immediate); N1 = 0 reads it from g.
+// L = columns per thread: each thread carries the same point of L columns
+// (own plane ring and exchange arrays per column), so every per-thread cost
+// (addressing, branches, barriers, coefficient loads) is shared by L
+// right-hand sides and the L independent arithmetic chains interleave.
+template <typename T, typename TO, int MODE, int MAXT, int N1, int L>
 __global__ void __launch_bounds__(MAXT, 1)
 plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__ MarchGeom g,
                    const T *__restrict__ in, TO *__restrict__ out, ColumnSet cs,
                    double *__restrict__ partials, unsigned *__restrict__ err) {
-    const int col = blockIdx.x / g.ntiles;
+    const int grp = blockIdx.x / g.ntiles;
     const int tile = blockIdx.x % g.ntiles;
-    if (col >= cs.ncols) return;
-    if (cs.status && cs.status[col] != COL_ACTIVE) return;
-    if (cs.flag && !cs.flag[col]) return;
+    // Columns of this CTA; an inactive lane (past the end, not active, or not
+    // flagged) mirrors an active one's input and stores nothing.
+    int colv[L];
+    bool act[L];
+    int first = -1;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const int c = grp * L + l;
+        bool a = c < cs.ncols;
+        if (a && cs.status && cs.status[c] != COL_ACTIVE) a = false;
+        if (a && cs.flag && !cs.flag[c]) a = false;
+        colv[l] = c;
+        act[l] = a;
+        if (a && first < 0) first = c;
+    }
+    if (first < 0) return;
+#pragma unroll
+    for (int l = 0; l < L; ++l)
+        if (!act[l]) colv[l] = first;
 
-    const int n1 = g.n1, n2 = g.n2, n3 = g.n3;
+    const int n1 = N1 > 0 ? N1 : g.n1;
+    const int n2 = g.n2, n3 = g.n3;
     const int a0 = (int)((long long)tile * n2 / g.ntiles);
     const int a1 = (int)((long long)(tile + 1) * n2 / g.ntiles);
     constexpr int AE = 16 / (int)sizeof(T);  // elements per 16 bytes
@@ -225,10 +291,14 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smem_raw);
     volatile int *s_dead = reinterpret_cast<volatile int *>(smem_raw + 56);  // [2], by step parity
     double *red = reinterpret_cast<double *>(smem_raw + 64);
-    T *ring = reinterpret_cast<T *>(smem_raw + 64 + 32 * 8);
-    const int NP = 2 * n1 * g.t2max;  // points per tile
-    T *xF1 = ring + (size_t)EQD_NSLOT * 6 * g.CH;  // [2][NP], by step parity
-    T *xH21 = xF1 + 2 * NP;                        // [2][NP]
+    T *ring = reinterpret_cast<T *>(smem_raw + 64 + 32 * 8);  // [L][slot][side*3+comp][CH]
+    constexpr int CHc = N1 > 0 ? march_chcap(N1, MAXT, (int)sizeof(T)) : 0;
+    constexpr int NPc = N1 > 0 ? 2 * N1 * march_t2cap(N1, MAXT) : 0;
+    const int CH = N1 > 0 ? CHc : g.CH;                     // chunk capacity per (side, comp)
+    const int RS = EQD_NSLOT * 6 * CH;                        // ring size per column
+    const int NP = N1 > 0 ? NPc : 2 * n1 * g.t2max;           // exchange entries per parity
+    T *xF1 = ring + (size_t)L * RS;                           // [L][2 (step parity)][NP]
+    T *xH21 = xF1 + (size_t)L * 2 * NP;                       // [L][2][NP]
 
     // ---- thread -> point: warp-homogeneous classes --------------------------
     // class 0: x2-interior rows, not on the fault; class 1: x2-closure rows,
@@ -240,17 +310,17 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const int ihi = max(min(a1, n2 - 6), ilo);
     const int nI = ihi - ilo;
     const int per = 2 * (n1 - 1);
-    const int N0 = nI * per, N1 = (T2 - nI) * per, N2 = 2 * T2;
+    const int C0 = nI * per, C1 = (T2 - nI) * per, C2 = 2 * T2;  // threads per class
     int side = 0, i2 = a0, i1 = 0, cls = 3;
-    if (tid < N0) {
+    if (tid < C0) {
         const int rr = tid / per, q = tid % per;
         side = q / (n1 - 1);
         const int j = q % (n1 - 1);
         i1 = side == 0 ? j : j + 1;
         i2 = ilo + rr;
         cls = 0;
-    } else if (tid < N0 + N1) {
-        const int k = tid - N0;
+    } else if (tid < C0 + C1) {
+        const int k = tid - C0;
         const int rr = k / per, q = k % per;
         side = q / (n1 - 1);
         const int j = q % (n1 - 1);
@@ -258,8 +328,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         const int nlow = ilo - a0;
         i2 = rr < nlow ? a0 + rr : ihi + (rr - nlow);
         cls = 1;
-    } else if (tid < N0 + N1 + N2) {
-        const int k = tid - N0 - N1;
+    } else if (tid < C0 + C1 + C2) {
+        const int k = tid - C0 - C1;
         side = k & 1;
         i1 = side == 0 ? n1 - 1 : 0;
         i2 = a0 + (k >> 1);
@@ -272,14 +342,12 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const X2Corr gw = x2_geom(i2, n1, n2, 6);
     const unsigned facemask = __ballot_sync(0xffffffffu, is_face);
     const int i2l = i2 - a0;
-    const int pidx = (side * g.t2max + i2l) * n1 + i1;
+    const int t2cap = N1 > 0 ? march_t2cap(N1, MAXT) : g.t2max;
+    const int pidx = (side * t2cap + i2l) * n1 + i1;
 
-    const T *incol = in + (long long)col * g.colstride;
-    TO *outcol = out + (long long)col * g.colstride;
-
-    // Zero the ring (rows outside the domain must read as zero), init barriers.
+    // Zero the rings (rows outside the domain must read as zero), init barriers.
     {
-        const int nring = EQD_NSLOT * 6 * g.CH;
+        const int nring = L * RS;
         for (int i = tid; i < nring; i += blockDim.x) ring[i] = T(0);
         fence_proxy_async_smem();
         if (tid == 0) {
@@ -293,11 +361,15 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
     auto issue_plane = [&](int q) {
         const int slot = q % EQD_NSLOT;
-        mbar_arrive_expect_tx(&mbar[slot], 6u * bytes);
-        for (int sc = 0; sc < 6; ++sc) {
-            T *dst = ring + ((size_t)slot * 6 + sc) * g.CH + (e0 - base);
-            const T *src = incol + ((long long)sc * n3 + q) * g.PS + e0;
-            bulk_g2s(dst, src, bytes, &mbar[slot]);
+        mbar_arrive_expect_tx(&mbar[slot], (unsigned)L * 6u * bytes);
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            const T *incol = in + (long long)colv[l] * g.colstride;
+            for (int sc = 0; sc < 6; ++sc) {
+                T *dst = ring + (size_t)l * RS + ((size_t)slot * 6 + sc) * CH + (e0 - base);
+                const T *src = incol + ((long long)sc * n3 + q) * g.PS + e0;
+                bulk_g2s(dst, src, bytes, &mbar[slot]);
+            }
         }
     };
     int issued = min(EQD_NSLOT, n3);
@@ -341,23 +413,34 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const bool ff_x12 = (side == 0 && i1 == 0) || (side == 1 && i1 == n1 - 1) || i2 == 0 || i2 == n2 - 1;
     const T wq1 = (i1 < 4) ? A1.wq[i1] : (i1 >= n1 - 4 ? A1.wq[n1 - 1 - i1] : T(1));
     const T wq2 = (i2 < 4) ? A2.wq[i2] : (i2 >= n2 - 4 ? A2.wq[n2 - 1 - i2] : T(1));
-    const T hpt = (T)(C.hvol * (double)wq1 * (double)wq2 * (MODE == MODE_RHS ? 1.0 : -1.0));
+    // H weight of this (x1, x2) point with the sign of the mode; zero on the
+    // x1/x2 far-field boundaries (P zeroes those rows).
+    const T hpt = ff_x12 ? T(0) : (T)(C.hvol * (double)wq1 * (double)wq2 * (MODE == MODE_RHS ? 1.0 : -1.0));
 
-    const int own = i2 * n1 + i1 - base;      // offset inside a chunk
-    const int lineoff = i2 * n1 + s1 - base;  // x1 window start
-    const long long ooff = (long long)i2 * n1 + i1;
+    const int own = i2 * n1 + i1 - base + side * 3 * CH;      // comp-0 offset inside a plane slot
+    const int lineoff = i2 * n1 + s1 - base + side * 3 * CH;  // comp-0 x1 window start
+    const long long cstr = (long long)n3 * g.PS;                // component stride in the column
+    const long long poff = (long long)(side * 3) * cstr + (long long)i2 * n1 + i1;
 
-    T v1w[7], v2w[7], v3w[7], F3w[7], H23w[7], w3q[7];
+    T v1w[L][7], v2w[L][7], v3w[L][7], F3w[L][7], H23w[L][7], w3q[L][4];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) v1w[k] = v2w[k] = v3w[k] = F3w[k] = H23w[k] = w3q[k] = T(0);
+    for (int l = 0; l < L; ++l) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) v1w[l][k] = v2w[l][k] = v3w[l][k] = F3w[l][k] = H23w[l][k] = T(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w3q[l][k] = T(0);
+    }
 
-    double acc0 = 0.0, acc1 = 0.0;
+    double acc0[L], acc1[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) acc0[l] = acc1[l] = 0.0;
     const T lam = C.lam, mu = C.mu, lpm = C.lpm, sat = C.sat_c;
     const int nsteps = n3 + 6;
     int dead_at = -1;
 
     // One march step. Windows are ordered by age: index 6 holds plane s,
-    // index 3 plane p = s - 3; the F3 and w3 queues hold p at 6, z = s - 6 at 3.
+    // index 3 plane p = s - 3; the F3 window holds p at 6 and z = s - 6 at 3;
+    // the w3 queue holds p at 3 and z at 0.
     auto step = [&](int s) -> bool {
         const int buf = s & 1;
         // ---- ingest plane s ----------------------------------------------------
@@ -366,148 +449,179 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             if (!mbar_wait_bounded(&mbar[slot], (unsigned)((s / EQD_NSLOT) & 1), err)) s_dead[buf] = 1;
             if (MODE != MODE_A) {
                 // Fix-up pass on the landed plane: chi (RHS) or P (generic input).
-                T *pl = ring + (size_t)slot * 6 * g.CH;
                 const int nrows = r1 - r0;
-                if (MODE == MODE_RHS) {
-                    if (s >= g.i3f0 && s < g.i3f0 + g.n3f) {
-                        for (int w = tid; w < nrows; w += blockDim.x) {
-                            const int r = r0 + w;
-                            if (r < g.i2f0 || r >= g.i2f0 + g.n2f) continue;
-                            const int k = (r - g.i2f0) + g.n2f * (s - g.i3f0);
-                            for (int j = 0; j < 2; ++j) {
-                                double sl;
-                                if (cs.slip_dense)
-                                    sl = cs.slip_dense[((long long)col * 2 + j) * g.nf + k];
-                                else
-                                    sl = (cs.slip_node[col] == k && cs.slip_comp[col] == j) ? 1.0 : 0.0;
-                                if (sl != 0.0) {
-                                    pl[(0 * 3 + 1 + j) * g.CH + r * n1 + (n1 - 1) - base] -= (T)(0.5 * sl);
-                                    pl[(1 * 3 + 1 + j) * g.CH + r * n1 + 0 - base] += (T)(0.5 * sl);
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    T *pl = ring + (size_t)l * RS + (size_t)slot * 6 * CH;
+                    const int col = colv[l];
+                    if (MODE == MODE_RHS) {
+                        if (s >= g.i3f0 && s < g.i3f0 + g.n3f) {
+                            for (int w = tid; w < nrows; w += blockDim.x) {
+                                const int r = r0 + w;
+                                if (r < g.i2f0 || r >= g.i2f0 + g.n2f) continue;
+                                const int k = (r - g.i2f0) + g.n2f * (s - g.i3f0);
+                                for (int j = 0; j < 2; ++j) {
+                                    double sl;
+                                    if (cs.slip_dense)
+                                        sl = cs.slip_dense[((long long)col * 2 + j) * g.nf + k];
+                                    else
+                                        sl = (cs.slip_node[col] == k && cs.slip_comp[col] == j) ? 1.0 : 0.0;
+                                    if (sl != 0.0) {
+                                        pl[(0 * 3 + 1 + j) * CH + r * n1 + (n1 - 1) - base] -= (T)(0.5 * sl);
+                                        pl[(1 * 3 + 1 + j) * CH + r * n1 + 0 - base] += (T)(0.5 * sl);
+                                    }
                                 }
                             }
                         }
-                    }
-                } else {  // MODE_AP: v = P x
-                    const bool plane_ff = (s == 0 || s == n3 - 1);
-                    for (int w = tid; w < nrows * 3; w += blockDim.x) {
-                        const int r = r0 + w / 3, j = w % 3;
-                        T *m = pl + (0 * 3 + j) * g.CH + r * n1 - base;
-                        T *pp = pl + (1 * 3 + j) * g.CH + r * n1 - base;
-                        if (plane_ff || r == 0 || r == n2 - 1) {
-                            for (int i = 0; i < n1; ++i) {
-                                m[i] = T(0);
-                                pp[i] = T(0);
+                    } else {  // MODE_AP: v = P x
+                        const bool plane_ff = (s == 0 || s == n3 - 1);
+                        for (int w = tid; w < nrows * 3; w += blockDim.x) {
+                            const int r = r0 + w / 3, j = w % 3;
+                            T *m = pl + (0 * 3 + j) * CH + r * n1 - base;
+                            T *pp = pl + (1 * 3 + j) * CH + r * n1 - base;
+                            if (plane_ff || r == 0 || r == n2 - 1) {
+                                for (int i = 0; i < n1; ++i) {
+                                    m[i] = T(0);
+                                    pp[i] = T(0);
+                                }
+                            } else {
+                                m[0] = T(0);
+                                pp[n1 - 1] = T(0);
+                                const T avg = T(0.5) * (m[n1 - 1] + pp[0]);
+                                m[n1 - 1] = avg;
+                                pp[0] = avg;
                             }
-                        } else {
-                            m[0] = T(0);
-                            pp[n1 - 1] = T(0);
-                            const T avg = T(0.5) * (m[n1 - 1] + pp[0]);
-                            m[n1 - 1] = avg;
-                            pp[0] = avg;
                         }
                     }
                 }
                 fence_proxy_async_smem();
                 __syncthreads();
             }
-            T a = T(0), b = T(0), c = T(0), h = T(0);
-            if (valid) {
-                const T *pl = ring + (size_t)slot * 6 * g.CH;
-                const T *c3 = pl + (side * 3 + 2) * g.CH + own;
-                a = pl[(side * 3 + 0) * g.CH + own];
-                b = pl[(side * 3 + 1) * g.CH + own];
-                c = c3[0];
-                h = x2_d1i(A2, c3, n1);
-                if (x2cl) x2_corr_d1(A2, gdd, c3, h);
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                T a = T(0), b = T(0), c = T(0), h = T(0);
+                if (valid) {
+                    const T *pl = ring + (size_t)l * RS + (size_t)slot * 6 * CH;
+                    const T *c3 = pl + 2 * CH + own;
+                    a = pl[own];
+                    b = pl[CH + own];
+                    c = c3[0];
+                    h = x2_d1i(A2, c3, n1);
+                    if (x2cl) x2_corr_d1(A2, gdd, c3, h);
+                }
+                push7(v1w[l], a);
+                push7(v2w[l], b);
+                push7(v3w[l], c);
+                push7(H23w[l], h);
             }
-            push7(v1w, a);
-            push7(v2w, b);
-            push7(v3w, c);
-            push7(H23w, h);
         } else {
-            push7(v1w, T(0));
-            push7(v2w, T(0));
-            push7(v3w, T(0));
-            push7(H23w, T(0));
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                push7(v1w[l], T(0));
+                push7(v2w[l], T(0));
+                push7(v3w[l], T(0));
+                push7(H23w[l], T(0));
+            }
         }
 
         // ---- in-plane work at p = s - 3 ---------------------------------------
         const int p = s - 3;
         const bool pin = p >= 0 && p < n3;
-        T w1 = T(0), w2 = T(0), w3p = T(0), F3 = T(0);
+        const bool x3i = p >= 4 && p <= n3 - 5;  // x3-interior plane (block-uniform)
+        const int r3 = p < 4 ? p : 4 + (n3 - 1 - p);
+        T w1[L], w2[L], w3p[L], F3[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) w1[l] = w2[l] = w3p[l] = F3[l] = T(0);
         if (valid && pin) {
-            const T *pl = ring + (size_t)(p % EQD_NSLOT) * 6 * g.CH;
-            const T *l1 = pl + (side * 3 + 0) * g.CH + lineoff;
-            const T *l2 = pl + (side * 3 + 1) * g.CH + lineoff;
-            const T *l3 = pl + (side * 3 + 2) * g.CH + lineoff;
-            const T *o1 = pl + (side * 3 + 0) * g.CH + own;
-            const T *o2 = pl + (side * 3 + 1) * g.CH + own;
-            const T *o3 = pl + (side * 3 + 2) * g.CH + own;
-            const T v1 = v1w[3], v2 = v2w[3], v3 = v3w[3];
-            T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const T x1 = l1[k], x2 = l2[k], x3 = l3[k];
-                G1 += c1[k] * x1;
-                A11 += c2[k] * x1;
-                A21 += c2[k] * x2;
-                A31 += c2[k] * x3;
-            }
-            T G2 = x2_d1i(A2, o2, n1);
-            T H21 = x2_d1i(A2, o1, n1);
-            T A12 = x2_d2i(A2, o1, v1, n1);
-            T A22 = x2_d2i(A2, o2, v2, n1);
-            T A32 = x2_d2i(A2, o3, v3, n1);
-            T W2 = x2_wi(A2, o2, v2, n1);
-            if (x2cl) {
-                T dummy = T(0);
-                x2_corr_dd(A2, gdd, o1, H21, A12);
-                x2_corr_dd(A2, gdd, o2, G2, A22);
-                x2_corr_dd(A2, gdd, o3, dummy, A32);
-                x2_corr_w(A2, gw, o2, W2);
-            }
-            const T G3 = x3_d1(A3, v3w, p, n3);
-            const T A13 = x3_d2(A3, v1w, p, n3);
-            const T A23 = x3_d2(A3, v2w, p, n3);
-            const T A33 = x3_d2(A3, v3w, p, n3);
-            const T D3H23 = x3_d1(A3, H23w, p, n3);
-            const T F1 = lam * G1 + lpm * (G2 + G3);
-            F3 = lam * G3 + lpm * (G1 + G2);
-            w1 = mu * (T(2) * A11 + A12 + A13);
-            w2 = mu * (A21 + T(2) * A22 + A23) + lam * W2 + lpm * D3H23;
-            w3p = mu * (A31 + A32 + T(2) * A33);
-            if (is_face) {
-                // Traction on the fixed +x1 axis (`traction_blocks`), with the
-                // +x1 boundary derivative of the fault node: lower end of the
-                // plus block (window cols 0..3), upper end of the minus block
-                // (window cols 5..2, odd mirror). SAT c (tau^+ - tau^-) on both
-                // faces; the partner (other side) is the adjacent lane.
-                T dh1 = T(0), dh2 = T(0), dh3 = T(0);
+            for (int l = 0; l < L; ++l) {
+                const T *pl = ring + (size_t)l * RS + (size_t)(p % EQD_NSLOT) * 6 * CH;
+                const T *l1 = pl + lineoff;
+                const T *l2 = l1 + CH;
+                const T *l3 = l2 + CH;
+                const T *o1 = pl + own;
+                const T *o2 = o1 + CH;
+                const T *o3 = o2 + CH;
+                const T v1 = v1w[l][3], v2 = v2w[l][3], v3 = v3w[l][3];
+                T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int q = side == 1 ? k : 5 - k;
-                    const T cf = side == 1 ? A1.dlo[k] : -A1.dlo[k];
-                    dh1 += cf * l1[q];
-                    dh2 += cf * l2[q];
-                    dh3 += cf * l3[q];
+                for (int k = 0; k < 6; ++k) {
+                    const T x1 = l1[k], x2 = l2[k], x3 = l3[k];
+                    G1 += c1[k] * x1;
+                    A11 += c2[k] * x1;
+                    A21 += c2[k] * x2;
+                    A31 += c2[k] * x3;
                 }
-                const T D3v1 = x3_d1(A3, v1w, p, n3);
-                const T tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
-                const T tau2 = mu * (H21 + dh2);
-                const T tau3 = mu * (D3v1 + dh3);
-                const T o1t = __shfl_xor_sync(facemask, tau1, 1);
-                const T o2t = __shfl_xor_sync(facemask, tau2, 1);
-                const T o3t = __shfl_xor_sync(facemask, tau3, 1);
-                const T sgn = side == 0 ? T(-1) : T(1);
-                w1 += sat * sgn * (tau1 - o1t);
-                w2 += sat * sgn * (tau2 - o2t);
-                w3p += sat * sgn * (tau3 - o3t);
+                T G2 = x2_d1i(A2, o2, n1);
+                T H21 = x2_d1i(A2, o1, n1);
+                T A12 = x2_d2i(A2, o1, v1, n1);
+                T A22 = x2_d2i(A2, o2, v2, n1);
+                T A32 = x2_d2i(A2, o3, v3, n1);
+                T W2 = x2_wi(A2, o2, v2, n1);
+                if (x2cl) {
+                    T dummy = T(0);
+                    x2_corr_dd(A2, gdd, o1, H21, A12);
+                    x2_corr_dd(A2, gdd, o2, G2, A22);
+                    x2_corr_dd(A2, gdd, o3, dummy, A32);
+                    x2_corr_w(A2, gw, o2, W2);
+                }
+                T G3, A13, A23, A33, D3H23;
+                if (x3i) {
+                    G3 = x3_d1i(A3, v3w[l]);
+                    A13 = x3_d2i(A3, v1w[l]);
+                    A23 = x3_d2i(A3, v2w[l]);
+                    A33 = x3_d2i(A3, v3w[l]);
+                    D3H23 = x3_d1i(A3, H23w[l]);
+                } else {
+                    G3 = x3_d1c(A3, v3w[l], r3);
+                    A13 = x3_d2c(A3, v1w[l], r3);
+                    A23 = x3_d2c(A3, v2w[l], r3);
+                    A33 = x3_d2c(A3, v3w[l], r3);
+                    D3H23 = x3_d1c(A3, H23w[l], r3);
+                }
+                const T F1 = lam * G1 + lpm * (G2 + G3);
+                F3[l] = lam * G3 + lpm * (G1 + G2);
+                w1[l] = mu * (T(2) * A11 + A12 + A13);
+                w2[l] = mu * (A21 + T(2) * A22 + A23) + lam * W2 + lpm * D3H23;
+                w3p[l] = mu * (A31 + A32 + T(2) * A33);
+                if (is_face) {
+                    // Traction on the fixed +x1 axis (`traction_blocks`), with the
+                    // +x1 boundary derivative of the fault node: lower end of the
+                    // plus block (window cols 0..3), upper end of the minus block
+                    // (window cols 5..2, odd mirror). SAT c (tau^+ - tau^-) on both
+                    // faces; the partner (other side) is the adjacent lane.
+                    T dh1 = T(0), dh2 = T(0), dh3 = T(0);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int q = side == 1 ? k : 5 - k;
+                        const T cf = side == 1 ? A1.dlo[k] : -A1.dlo[k];
+                        dh1 += cf * l1[q];
+                        dh2 += cf * l2[q];
+                        dh3 += cf * l3[q];
+                    }
+                    const T D3v1 = x3i ? x3_d1i(A3, v1w[l]) : x3_d1c(A3, v1w[l], r3);
+                    const T tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
+                    const T tau2 = mu * (H21 + dh2);
+                    const T tau3 = mu * (D3v1 + dh3);
+                    const T o1t = __shfl_xor_sync(facemask, tau1, 1);
+                    const T o2t = __shfl_xor_sync(facemask, tau2, 1);
+                    const T o3t = __shfl_xor_sync(facemask, tau3, 1);
+                    const T sgn = side == 0 ? T(-1) : T(1);
+                    w1[l] += sat * sgn * (tau1 - o1t);
+                    w2[l] += sat * sgn * (tau2 - o2t);
+                    w3p[l] += sat * sgn * (tau3 - o3t);
+                }
+                xF1[((size_t)l * 2 + buf) * NP + pidx] = F1;
+                xH21[((size_t)l * 2 + buf) * NP + pidx] = H21;
             }
-            xF1[buf * NP + pidx] = F1;
-            xH21[buf * NP + pidx] = H21;
         }
-        push7(F3w, F3);
-        push7(w3q, w3p);
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            push7(F3w[l], F3[l]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) w3q[l][k] = w3q[l][k + 1];
+            w3q[l][3] = w3p[l];
+        }
         __syncthreads();
         if (s_dead[buf]) {
             dead_at = s;
@@ -521,58 +635,63 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
         // ---- finish p: x1 derivatives of F1, H21; P, H; store -----------------
         if (valid && pin) {
-            const T *xf = xF1 + buf * NP + (pidx - i1 + s1);
-            const T *xh = xH21 + buf * NP + (pidx - i1 + s1);
-            T E1 = T(0), E21 = T(0);
+            const T hw = hpt * plane_weight(A3, p, n3);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                E1 += c1[k] * xf[k];
-                E21 += c1[k] * xh[k];
-            }
-            w1 += E1;
-            w2 += lpm * E21;
-            if (is_face) {
-                w1 = T(0.5) * (w1 + __shfl_xor_sync(facemask, w1, 1));
-                w2 = T(0.5) * (w2 + __shfl_xor_sync(facemask, w2, 1));
-            }
-            const bool ff = ff_x12 || p == 0 || p == n3 - 1;
-            const int rq = p < 4 ? p : (p >= n3 - 4 ? n3 - 1 - p : -1);
-            const T hw = ff ? T(0) : hpt * (rq >= 0 ? A3.wq[rq] : T(1));
-            const T y1 = hw * w1, y2 = hw * w2;
-            const long long o = ((long long)(side * 3 + 0) * n3 + p) * g.PS + ooff;
-            outcol[o] = (TO)y1;
-            outcol[o + (long long)n3 * g.PS] = (TO)y2;
-            const T va = v1w[3], vb = v2w[3];
-            if (MODE == MODE_RHS) {
-                acc0 += (double)y1 * (double)y1 + (double)y2 * (double)y2;
-            } else if (sizeof(T) == 4) {
-                acc0 += (double)(va * y1 + vb * y2);
-                acc1 += (double)(va * va + vb * vb);
-            } else {
-                acc0 += (double)va * (double)y1 + (double)vb * (double)y2;
-                acc1 += (double)va * (double)va + (double)vb * (double)vb;
+            for (int l = 0; l < L; ++l) {
+                const T *xf = xF1 + ((size_t)l * 2 + buf) * NP + (pidx - i1 + s1);
+                const T *xh = xH21 + ((size_t)l * 2 + buf) * NP + (pidx - i1 + s1);
+                T E1 = T(0), E21 = T(0);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    E1 += c1[k] * xf[k];
+                    E21 += c1[k] * xh[k];
+                }
+                T u1 = w1[l] + E1;
+                T u2 = w2[l] + lpm * E21;
+                if (is_face) {
+                    u1 = T(0.5) * (u1 + __shfl_xor_sync(facemask, u1, 1));
+                    u2 = T(0.5) * (u2 + __shfl_xor_sync(facemask, u2, 1));
+                }
+                const T y1 = hw * u1, y2 = hw * u2;
+                if (act[l]) {
+                    TO *o = out + (long long)colv[l] * g.colstride + poff + (long long)p * g.PS;
+                    o[0] = (TO)y1;
+                    o[cstr] = (TO)y2;
+                }
+                const T va = v1w[l][3], vb = v2w[l][3];
+                if (MODE == MODE_RHS) {
+                    acc0[l] += (double)y1 * (double)y1 + (double)y2 * (double)y2;
+                } else if (sizeof(T) == 4) {
+                    acc0[l] += (double)(va * y1 + vb * y2);
+                    acc1[l] += (double)(va * va + vb * vb);
+                } else {
+                    acc0[l] += (double)va * (double)y1 + (double)vb * (double)y2;
+                    acc1[l] += (double)va * (double)va + (double)vb * (double)vb;
+                }
             }
         }
         // ---- finish z = s - 6: comp 3 --------------------------------------------
         const int z = s - 6;
         if (valid && z >= 0 && z < n3) {
-            T w3 = w3q[3] + x3_d1(A3, F3w, z, n3);
-            if (is_face) w3 = T(0.5) * (w3 + __shfl_xor_sync(facemask, w3, 1));
-            const bool ff = ff_x12 || z == 0 || z == n3 - 1;
-            const int rq = z < 4 ? z : (z >= n3 - 4 ? n3 - 1 - z : -1);
-            const T hw = ff ? T(0) : hpt * (rq >= 0 ? A3.wq[rq] : T(1));
-            const T y3 = hw * w3;
-            const long long o = ((long long)(side * 3 + 2) * n3 + z) * g.PS + ooff;
-            outcol[o] = (TO)y3;
-            const T vc = v3w[0];
-            if (MODE == MODE_RHS) {
-                acc0 += (double)y3 * (double)y3;
-            } else if (sizeof(T) == 4) {
-                acc0 += (double)(vc * y3);
-                acc1 += (double)(vc * vc);
-            } else {
-                acc0 += (double)vc * (double)y3;
-                acc1 += (double)vc * (double)vc;
+            const T hw = hpt * plane_weight(A3, z, n3);
+            const bool x3iz = z >= 4 && z <= n3 - 5;
+            const int r3z = z < 4 ? z : 4 + (n3 - 1 - z);
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                T w3 = w3q[l][0] + (x3iz ? x3_d1i(A3, F3w[l]) : x3_d1c(A3, F3w[l], r3z));
+                if (is_face) w3 = T(0.5) * (w3 + __shfl_xor_sync(facemask, w3, 1));
+                const T y3 = hw * w3;
+                if (act[l]) out[(long long)colv[l] * g.colstride + poff + 2 * cstr + (long long)z * g.PS] = (TO)y3;
+                const T vc = v3w[l][0];
+                if (MODE == MODE_RHS) {
+                    acc0[l] += (double)y3 * (double)y3;
+                } else if (sizeof(T) == 4) {
+                    acc0[l] += (double)(vc * y3);
+                    acc1[l] += (double)(vc * vc);
+                } else {
+                    acc0[l] += (double)vc * (double)y3;
+                    acc1[l] += (double)vc * (double)vc;
+                }
             }
         }
         return true;
@@ -593,13 +712,17 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         return;
     }
 
-    const double s0 = block_sum(acc0, red);
-    __syncthreads();
-    const double s1v = block_sum(acc1, red);
-    if (tid == 0 && partials) {
-        double *pp = partials + ((long long)col * g.ntiles + tile) * 2;
-        pp[0] = s0;
-        pp[1] = s1v;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const double s0 = block_sum(acc0[l], red);
+        __syncthreads();
+        const double s1v = block_sum(acc1[l], red);
+        __syncthreads();
+        if (tid == 0 && partials && act[l]) {
+            double *pp = partials + ((long long)colv[l] * g.ntiles + tile) * 2;
+            pp[0] = s0;
+            pp[1] = s1v;
+        }
     }
 }
 

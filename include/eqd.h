@@ -88,7 +88,7 @@ typedef struct {
     int32_t precond;          /* eqd_precond */
     int32_t precision;        /* eqd_precision */
     int32_t chunk;            /* columns per device batch; 0 -> as many as the HBM budget allows */
-    double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.1) */
+    double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.01) */
     uint64_t hbm_budget_bytes;/* 0 -> free device memory minus 2 GiB */
     int32_t tile_rows;        /* x2 rows per CTA tile in the stencil; 0 -> autotuned */
     uint32_t flags;

@@ -85,9 +85,22 @@ def test_reference_fault_response_suite(eqd):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_batched_equals_single(eqd, precision):
+    _batched_equals_single(eqd, precision, None)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_batched_equals_single_every_variant(eqd, variant):
+    """Bit-identity holds for every stencil launch variant, including the
+    two-columns-per-thread ones (a column's partner lane must not matter)."""
+    _batched_equals_single(eqd, "mixed", variant)
+
+
+def _batched_equals_single(eqd, precision, variant):
     """A column computed in a batch is bit-identical to the same column alone
     (the reference's `threaded K build matches serial`, :100-112)."""
     fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4, precision=precision)
+    if variant is not None:
+        eqd.set_stencil_variant(fe, variant)
     cols = np.arange(2 * fe.nf)
     Kb, itb, stb = eqd.stiffness_columns(fe, cols)
     for c in (0, 7, fe.nf + 3):
