@@ -232,6 +232,9 @@ def main():
     time.sleep(0.3)
     torch.cuda.synchronize()
     dev_s, launches, step_ms, iters = [], 0, [], 0
+    # Profiler brackets: under `ncu --profile-from-start off` only the timed
+    # steps' launches are captured (no-ops otherwise).
+    torch.cuda.profiler.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = device_step()
@@ -241,6 +244,7 @@ def main():
         iters += st.iterations
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
+    torch.cuda.profiler.stop()
     clocks = clk.stop()
     barrier(world)
     dev_total = barrier_max(world, float(sum(dev_s)))
