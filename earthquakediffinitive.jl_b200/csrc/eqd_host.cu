@@ -149,13 +149,12 @@ struct Workspace {
     DevBuf gamma, beta, rr_ref, tol, bnorm, iters, status, flag;
     DevBuf slip_node, slip_comp, slip_dense;
     DevBuf kout;
-    DevBuf active;
-    int *h_active = nullptr;
+    DevBuf newmask, slot_list, dst_list;  // slot engine: entering columns, extraction lists
+    DevBuf hbuf;                          // explicit-RHS staging (reference layout)
     cudaGraphExec_t graph = nullptr;
     int graph_cap = -1, graph_prec = -1, graph_iters = 0, graph_generic = -1, graph_sel = -1;
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
-        if (h_active) cudaFreeHost(h_active);
     }
 };
 
@@ -627,215 +626,390 @@ static void record_iteration(eqd_grid *G, Workspace &W, int cap, int mixed, int 
     cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(p, r, st, sp);
 }
 
+// ---------------------------------------------------------------------------
+// Slot engine: a fixed set of column slots, each holding one right-hand side's
+// CG state. A column enters a free slot (its vectors are zeroed and r0 = b is
+// evaluated for it alone), runs with every other occupied slot in the
+// graph-captured iterations, and leaves when its status is final; its slot is
+// then free for the next column. A column's arithmetic does not depend on the
+// other slots (every reduction is per column, in a fixed order), so a column
+// gives the same bits whenever and beside whatever it runs.
+// ---------------------------------------------------------------------------
+struct ColWork {
+    int slip_node = -1;                  // unit slip at this Omega_f node (-1: none)
+    int slip_comp = 0;                   // 0 -> s2, 1 -> s3
+    const double *slip_dense = nullptr;  // host [2][nf] slip field, or null
+    const double *rhs = nullptr;         // host reference-layout right-hand side (explicit-RHS solve), or null
+    long long tag = 0;                   // the caller's id for the column
+};
+
+struct ColDone {
+    long long tag;
+    int slot;
+    int iters;
+    int8_t status;
+};
+
+template <typename T>
+struct SlotRun {
+    eqd_grid *G = nullptr;
+    Workspace *W = nullptr;
+    int cap = 0, mixed = 0, generic = 0, dense = 0;
+    long long itmax = 0;
+    SolveParams sp{};
+    ColState st{};
+    std::vector<int> hn, hc, hit, hslot, hdst;
+    std::vector<int8_t> hst, hnew;
+    std::vector<long long> tag;  // -1: free slot
+    int held = 0;                // occupied slots (running or finished, not yet released)
+    int64_t launches = 0;
+    static constexpr int kIter = 10;
+
+    int setup(eqd_grid *g, const eqd_solve_opts &o, int capacity, bool gen, bool dns) {
+        G = g;
+        W = &G->ws;
+        cap = capacity;
+        mixed = o.precision == EQD_PREC_MIXED;
+        generic = gen;
+        dense = dns;
+        const GridConst &gc = G->gc;
+        const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
+        const size_t vec = (size_t)gc.colstride * cap;
+        if (mixed && !G->tuned) {
+            int rc = tune_variants(G, std::min(cap, 512));
+            if (rc) return rc;
+        }
+        const int nt32 = G->v32[G->sel32].g.ntiles, nt64 = G->m64.g.ntiles;
+        Workspace &w = *W;
+        CUDA_OR_RETURN(w.x64.ensure(sizeof(double) * vec));
+        CUDA_OR_RETURN(w.v0.ensure(sizeof(T) * vec));
+        CUDA_OR_RETURN(w.v1.ensure(sizeof(T) * vec));
+        CUDA_OR_RETURN(w.v2.ensure(sizeof(T) * vec));
+        if (mixed) CUDA_OR_RETURN(w.v3.ensure(sizeof(float) * vec));
+        int ntmax = std::max(nt64, G->m32.g.ntiles);
+        for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
+        CUDA_OR_RETURN(w.apply_part.ensure(sizeof(double) * 2 * cap * ntmax));
+        CUDA_OR_RETURN(w.res_part.ensure(sizeof(double) * 2 * cap * std::max(nt64, G->nchunks)));
+        CUDA_OR_RETURN(w.rr_part.ensure(sizeof(double) * cap * G->nchunks));
+        for (DevBuf *b : {&w.gamma, &w.beta, &w.rr_ref, &w.tol, &w.bnorm}) CUDA_OR_RETURN(b->ensure(sizeof(double) * cap));
+        CUDA_OR_RETURN(w.iters.ensure(sizeof(int) * cap));
+        CUDA_OR_RETURN(w.status.ensure(cap));
+        CUDA_OR_RETURN(w.flag.ensure(cap));
+        CUDA_OR_RETURN(w.newmask.ensure(cap));
+        CUDA_OR_RETURN(w.slot_list.ensure(sizeof(int) * cap));
+        CUDA_OR_RETURN(w.dst_list.ensure(sizeof(int) * cap));
+        CUDA_OR_RETURN(w.slip_node.ensure(sizeof(int) * cap));
+        CUDA_OR_RETURN(w.slip_comp.ensure(sizeof(int) * cap));
+        if (dense) CUDA_OR_RETURN(w.slip_dense.ensure(sizeof(double) * 2 * gc.nf * cap));
+        else w.slip_dense.release();
+        CUDA_OR_RETURN(w.kout.ensure(sizeof(double) * 2 * gc.nf * cap));
+        if (generic) CUDA_OR_RETURN(w.hbuf.ensure(sizeof(double) * ntot * cap));
+
+        st = ColState{w.gamma.as<double>(), w.beta.as<double>(), w.rr_ref.as<double>(), w.tol.as<double>(),
+                      w.bnorm.as<double>(), w.iters.as<int>(), w.status.as<int8_t>(), w.flag.as<int8_t>()};
+        sp = SolveParams{};
+        sp.rtol = o.rtol;
+        sp.atol = o.atol;
+        sp.itmax = o.itmax;
+        sp.delta = o.reliable_delta > 0 ? o.reliable_delta : 0.01;
+        sp.ntiles = sizeof(T) == 4 ? nt32 : nt64;
+        sp.nchunks = G->nchunks;
+        sp.colstride = gc.colstride;
+        sp.ntot = ntot;
+        itmax = o.itmax > 0 ? o.itmax : 2 * ntot;
+
+        // Every slot starts free: status IDLE everywhere, vectors zeroed as
+        // columns enter.
+        hn.assign(cap, -1);
+        hc.assign(cap, 0);
+        hit.assign(cap, 0);
+        hst.assign(cap, (int8_t)COL_IDLE);
+        hnew.assign(cap, 0);
+        tag.assign(cap, -1);
+        hslot.resize(cap);
+        hdst.resize(cap);
+        held = 0;
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.status.p, hst.data(), cap, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemsetAsync(w.flag.p, 0, cap, G->stream));
+
+        // Graph of kIter iterations over all slots, captured once per
+        // (capacity, precision, mode, launch variant).
+        if (!w.graph || w.graph_cap != cap || w.graph_prec != o.precision || w.graph_generic != generic ||
+            w.graph_sel != G->sel32) {
+            if (w.graph) cudaGraphExecDestroy(w.graph);
+            w.graph = nullptr;
+            cudaGraph_t g;
+            CUDA_OR_RETURN(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < kIter; ++k) record_iteration<T>(G, w, cap, mixed, generic, sp, st);
+            cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
+            if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&w.graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            w.graph_cap = cap;
+            w.graph_prec = o.precision;
+            w.graph_generic = generic;
+            w.graph_sel = G->sel32;
+            w.graph_iters = kIter;
+        }
+        return EQD_OK;
+    }
+
+    int free_slots() const { return cap - held; }
+
+    ColumnSet colset() const {
+        ColumnSet cs{};
+        cs.ncols = cap;
+        cs.slip_node = W->slip_node.as<int>();
+        cs.slip_comp = W->slip_comp.as<int>();
+        cs.slip_dense = dense ? W->slip_dense.as<double>() : nullptr;
+        cs.status = W->status.as<int8_t>();
+        return cs;
+    }
+
+    // Put up to n columns into free slots and evaluate their r0 = b; `taken`
+    // is how many entered.
+    int admit(const ColWork *work, int n, int &taken) {
+        taken = 0;
+        const GridConst &gc = G->gc;
+        const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
+        Workspace &w = *W;
+        std::fill(hnew.begin(), hnew.end(), (int8_t)0);
+        for (int s = 0; s < cap && taken < n; ++s) {
+            if (tag[s] >= 0) continue;
+            const ColWork &c = work[taken++];
+            tag[s] = c.tag;
+            hn[s] = c.slip_node;
+            hc[s] = c.slip_comp;
+            hst[s] = COL_ACTIVE;
+            hit[s] = 0;
+            hnew[s] = 1;
+            ++held;
+            if (dense) {
+                if (c.slip_dense)
+                    CUDA_OR_RETURN(cudaMemcpyAsync(w.slip_dense.as<double>() + (size_t)s * 2 * gc.nf, c.slip_dense,
+                                                   sizeof(double) * 2 * gc.nf, cudaMemcpyHostToDevice, G->stream));
+                else
+                    CUDA_OR_RETURN(cudaMemsetAsync(w.slip_dense.as<double>() + (size_t)s * 2 * gc.nf, 0,
+                                                   sizeof(double) * 2 * gc.nf, G->stream));
+            }
+        }
+        if (taken == 0) return EQD_OK;
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.slip_node.p, hn.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.slip_comp.p, hc.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.status.p, hst.data(), cap, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.iters.p, hit.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.newmask.p, hnew.data(), cap, cudaMemcpyHostToDevice, G->stream));
+        const int8_t *mask = w.newmask.as<int8_t>();
+        const unsigned nb = (unsigned)(cap * G->nchunks);
+        const long long cst = gc.colstride;
+        zero_columns_kernel<double><<<nb, 256, 0, G->stream>>>(w.x64.as<double>(), cst, G->nchunks, mask);
+        zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v0.as<T>(), cst, G->nchunks, mask);
+        zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), cst, G->nchunks, mask);
+        zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v2.as<T>(), cst, G->nchunks, mask);
+        if (mixed) zero_columns_kernel<float><<<nb, 256, 0, G->stream>>>(w.v3.as<float>(), cst, G->nchunks, mask);
+        launches += mixed ? 5 : 4;
+        const unsigned sb = (unsigned)((cap + 127) / 128);
+        if (!generic) {
+            // r0 = b = H P (D+SAT) chi  (x = 0), in the working precision.
+            ColumnSet cs = colset();
+            cs.flag = mask;
+            CUDA_OR_RETURN((launch_march<double, T, MODE_RHS>(G, w.x64.as<double>(), w.v0.as<T>(), cs,
+                                                               w.res_part.as<double>(), cap)));
+            SolveParams sp2 = sp;
+            sp2.ntiles = G->m64.g.ntiles;
+            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, w.res_part.as<double>(), cap, mixed, mask);
+            launches += 2;
+        } else {
+            // r0 = b given explicitly (reference layout, FP64).
+            int j = 0;
+            for (int s = 0; s < cap && j < taken; ++s) {
+                if (!hnew[s]) continue;
+                const ColWork &c = work[j++];
+                double *hb = w.hbuf.as<double>() + (size_t)s * ntot;
+                CUDA_OR_RETURN(cudaMemcpyAsync(hb, c.rhs, sizeof(double) * ntot, cudaMemcpyHostToDevice, G->stream));
+                const int tb = 256;
+                ref_to_dev_kernel<double, T><<<(unsigned)((ntot + tb - 1) / tb), tb, 0, G->stream>>>(
+                    hb, w.v0.as<T>() + (size_t)s * gc.colstride, gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, 1);
+                ++launches;
+            }
+            column_sumsq_kernel<T><<<nb, 256, 0, G->stream>>>(w.v0.as<T>(), cst, G->nchunks, mask,
+                                                               w.res_part.as<double>());
+            SolveParams sp2 = sp;
+            sp2.ntiles = G->nchunks;
+            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, w.res_part.as<double>(), cap, 0, mask);
+            launches += 2;
+        }
+        cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), w.v0.as<T>(), st, sp, mask);
+        ++launches;
+        CUDA_OR_RETURN(cudaGetLastError());
+        return EQD_OK;
+    }
+
+    // Run kIter iterations (when a column is running), then list the occupied
+    // slots whose status is final.
+    int advance(std::vector<ColDone> &done) {
+        done.clear();
+        Workspace &w = *W;
+        int running = 0;
+        for (int s = 0; s < cap; ++s) running += tag[s] >= 0 && hst[s] == COL_ACTIVE;
+        if (running > 0) {
+            CUDA_OR_RETURN(cudaGraphLaunch(w.graph, G->stream));
+            launches += (int64_t)kIter * (mixed ? 7 : 4);
+        }
+        CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), w.status.p, cap, cudaMemcpyDeviceToHost, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), w.iters.p, sizeof(int) * cap, cudaMemcpyDeviceToHost, G->stream));
+        CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+        int rc = check_device_error(G);
+        if (rc) return rc;
+        bool forced = false;
+        for (int s = 0; s < cap; ++s) {
+            if (tag[s] < 0) continue;
+            if (hst[s] == COL_ACTIVE && hit[s] > itmax + 2 * kIter) {  // defensive: the kernels stop at itmax
+                hst[s] = COL_MAXITER;
+                forced = true;
+            }
+            if (hst[s] != COL_ACTIVE) done.push_back(ColDone{tag[s], s, hit[s], hst[s]});
+        }
+        if (forced)
+            CUDA_OR_RETURN(cudaMemcpyAsync(w.status.p, hst.data(), cap, cudaMemcpyHostToDevice, G->stream));
+        return EQD_OK;
+    }
+
+    // K columns of finished slots: into K (device) at column dst (the tag when
+    // `to_tag`, else the position in `done`), leading dimension kld.
+    int extract(const std::vector<ColDone> &done, double *K, long long kld, bool to_tag) {
+        if (done.empty()) return EQD_OK;
+        const GridConst &gc = G->gc;
+        Workspace &w = *W;
+        const int n = (int)done.size();
+        for (int j = 0; j < n; ++j) {
+            hslot[j] = done[j].slot;
+            hdst[j] = to_tag ? (int)done[j].tag : j;
+        }
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.slot_list.p, hslot.data(), sizeof(int) * n, cudaMemcpyHostToDevice, G->stream));
+        CUDA_OR_RETURN(cudaMemcpyAsync(w.dst_list.p, hdst.data(), sizeof(int) * n, cudaMemcpyHostToDevice, G->stream));
+        ExtractGeom eg{gc.n1, gc.n2, gc.n3, gc.PS, gc.nf, gc.i2f0, gc.n2f, gc.i3f0, gc.n3f, gc.colstride, gc.mu};
+        const long long nthr = (long long)n * gc.nf;
+        extract_traction_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, G->stream>>>(
+            G->c64, eg, w.x64.as<double>(), colset(), K, kld, n, w.slot_list.as<int>(), w.dst_list.as<int>());
+        ++launches;
+        CUDA_OR_RETURN(cudaGetLastError());
+        return EQD_OK;
+    }
+
+    // Explicit-RHS solve: the solution of a finished slot in reference layout.
+    int solution(int slot, double *host_u) {
+        const GridConst &gc = G->gc;
+        const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
+        Workspace &w = *W;
+        double *hb = w.hbuf.as<double>() + (size_t)slot * ntot;
+        const int tb = 256;
+        dev_to_ref_kernel<double, double><<<(unsigned)((ntot + tb - 1) / tb), tb, 0, G->stream>>>(
+            w.x64.as<double>() + (size_t)slot * gc.colstride, hb, gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, 1);
+        ++launches;
+        CUDA_OR_RETURN(cudaMemcpyAsync(host_u, hb, sizeof(double) * ntot, cudaMemcpyDeviceToHost, G->stream));
+        return EQD_OK;
+    }
+
+    // Free the slots of finished columns.
+    int release(const std::vector<ColDone> &done) {
+        if (done.empty()) return EQD_OK;
+        for (const ColDone &d : done) {
+            tag[d.slot] = -1;
+            hn[d.slot] = -1;
+            hst[d.slot] = COL_IDLE;
+            --held;
+        }
+        CUDA_OR_RETURN(cudaMemcpyAsync(W->status.p, hst.data(), cap, cudaMemcpyHostToDevice, G->stream));
+        return EQD_OK;
+    }
+};
+
+// Batched solve through the slot engine: columns enter as slots free up; K
+// columns go to the caller's device or host buffer as each column finishes.
 template <typename T>
 static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, eqd_stats *stats) {
     const GridConst &gc = G->gc;
-    const int mixed = o.precision == EQD_PREC_MIXED;
     const int generic = B.rhs != nullptr;
     const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
     int chunk = 0;
     int rc = resolve_chunk(G, o, B.ncols, o.precision, chunk);
     if (rc) return rc;
-    Workspace &W = G->ws;
-    const size_t vec = (size_t)gc.colstride * chunk;
-    if (mixed && !G->tuned) {
-        rc = tune_variants(G, std::min(chunk, 512));
-        if (rc) return rc;
+    SlotRun<T> R;
+    rc = R.setup(G, o, chunk, generic, B.slip_dense != nullptr);
+    if (rc) return rc;
+
+    std::vector<ColWork> work(B.ncols);
+    for (int i = 0; i < B.ncols; ++i) {
+        ColWork &c = work[i];
+        c.tag = i;
+        c.slip_node = B.slip_node ? B.slip_node[i] : -1;
+        c.slip_comp = B.slip_comp ? B.slip_comp[i] : 0;
+        c.slip_dense = B.slip_dense ? B.slip_dense + (size_t)i * 2 * gc.nf : nullptr;
+        c.rhs = B.rhs ? B.rhs + (size_t)i * ntot : nullptr;
     }
-    const int nt32 = G->v32[G->sel32].g.ntiles, nt64 = G->m64.g.ntiles;
-    const int ntA = sizeof(T) == 4 ? nt32 : nt64;
-    CUDA_OR_RETURN(W.x64.ensure(sizeof(double) * vec));
-    CUDA_OR_RETURN(W.v0.ensure(sizeof(T) * vec));
-    CUDA_OR_RETURN(W.v1.ensure(sizeof(T) * vec));
-    CUDA_OR_RETURN(W.v2.ensure(sizeof(T) * vec));
-    if (mixed) CUDA_OR_RETURN(W.v3.ensure(sizeof(float) * vec));
-    int ntmax = std::max(nt64, G->m32.g.ntiles);
-    for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
-    CUDA_OR_RETURN(W.apply_part.ensure(sizeof(double) * 2 * chunk * ntmax));
-    CUDA_OR_RETURN(W.res_part.ensure(sizeof(double) * 2 * chunk * std::max(nt64, G->nchunks)));
-    CUDA_OR_RETURN(W.rr_part.ensure(sizeof(double) * chunk * G->nchunks));
-    for (DevBuf *b : {&W.gamma, &W.beta, &W.rr_ref, &W.tol, &W.bnorm}) CUDA_OR_RETURN(b->ensure(sizeof(double) * chunk));
-    CUDA_OR_RETURN(W.iters.ensure(sizeof(int) * chunk));
-    CUDA_OR_RETURN(W.status.ensure(chunk));
-    CUDA_OR_RETURN(W.flag.ensure(chunk));
-    CUDA_OR_RETURN(W.slip_node.ensure(sizeof(int) * chunk));
-    CUDA_OR_RETURN(W.slip_comp.ensure(sizeof(int) * chunk));
-    if (B.slip_dense) CUDA_OR_RETURN(W.slip_dense.ensure(sizeof(double) * 2 * gc.nf * chunk));
-    else W.slip_dense.release();
-    CUDA_OR_RETURN(W.kout.ensure(sizeof(double) * 2 * gc.nf * chunk));
-    CUDA_OR_RETURN(W.active.ensure(sizeof(int)));
-    if (!W.h_active) CUDA_OR_RETURN(cudaHostAlloc(&W.h_active, sizeof(int), cudaHostAllocDefault));
-    DevBuf hbuf;
-    if (generic) CUDA_OR_RETURN(hbuf.ensure(sizeof(double) * ntot * chunk));
-
-    ColState st{W.gamma.as<double>(), W.beta.as<double>(), W.rr_ref.as<double>(), W.tol.as<double>(),
-                W.bnorm.as<double>(), W.iters.as<int>(), W.status.as<int8_t>(), W.flag.as<int8_t>()};
-    SolveParams sp{};
-    sp.rtol = o.rtol;
-    sp.atol = o.atol;
-    sp.itmax = o.itmax;
-    sp.delta = o.reliable_delta > 0 ? o.reliable_delta : 0.01;
-    sp.ntiles = ntA;
-    sp.nchunks = G->nchunks;
-    sp.colstride = gc.colstride;
-    sp.ntot = ntot;
-
-    // Graph of a few iterations, captured once per (chunk, precision, mode).
-    const int kIter = 10;
-    if (!W.graph || W.graph_cap != chunk || W.graph_prec != o.precision || W.graph_generic != generic ||
-        W.graph_sel != G->sel32) {
-        if (W.graph) cudaGraphExecDestroy(W.graph);
-        W.graph = nullptr;
-        cudaGraph_t g;
-        CUDA_OR_RETURN(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < kIter; ++k) record_iteration<T>(G, W, chunk, mixed, generic, sp, st);
-        cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
-        if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&W.graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-        W.graph_cap = chunk;
-        W.graph_prec = o.precision;
-        W.graph_generic = generic;
-        W.graph_sel = G->sel32;
-        W.graph_iters = kIter;
-    }
-
-    int64_t tot_it = 0, max_it = 0, unconv = 0, reliable = 0, launches = 0;
-    const int per_iter = mixed ? 7 : 4;
-    float dev_ms_total = 0.f;
-    std::vector<int> hn(chunk), hc(chunk), hit(chunk);
-    std::vector<int8_t> hst(chunk);
-    const int tb = 256;
-    for (int c0 = 0; c0 < B.ncols; c0 += chunk) {
-        const int nc = std::min(chunk, B.ncols - c0);
-        // Column descriptors (unused slots idle).
-        for (int i = 0; i < chunk; ++i) {
-            hn[i] = (i < nc && B.slip_node) ? B.slip_node[c0 + i] : -1;
-            hc[i] = (i < nc && B.slip_comp) ? B.slip_comp[c0 + i] : 0;
-            hst[i] = i < nc ? COL_ACTIVE : COL_IDLE;
+    int64_t tot_it = 0, max_it = 0, unconv = 0;
+    std::vector<double> kstage;
+    if (!generic && B.kcols && !B.kdev) kstage.resize((size_t)2 * gc.nf * chunk);
+    CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+    int next = 0, finished = 0;
+    std::vector<ColDone> done;
+    while (finished < B.ncols) {
+        // Explicit-RHS solves refill only an empty engine (their staging
+        // buffer holds one wave of right-hand sides).
+        if (next < B.ncols && R.free_slots() > 0 && (!generic || R.held == 0)) {
+            int taken = 0;
+            rc = R.admit(work.data() + next, B.ncols - next, taken);
+            if (rc) return rc;
+            next += taken;
         }
-        CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_node.p, hn.data(), sizeof(int) * chunk, cudaMemcpyHostToDevice, G->stream));
-        CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_comp.p, hc.data(), sizeof(int) * chunk, cudaMemcpyHostToDevice, G->stream));
-        CUDA_OR_RETURN(cudaMemcpyAsync(W.status.p, hst.data(), chunk, cudaMemcpyHostToDevice, G->stream));
-        if (B.slip_dense) {
-            CUDA_OR_RETURN(cudaMemsetAsync(W.slip_dense.p, 0, sizeof(double) * 2 * gc.nf * chunk, G->stream));
-            CUDA_OR_RETURN(cudaMemcpyAsync(W.slip_dense.p, B.slip_dense + (size_t)c0 * 2 * gc.nf,
-                                           sizeof(double) * 2 * gc.nf * nc, cudaMemcpyHostToDevice, G->stream));
-        }
-        CUDA_OR_RETURN(cudaMemsetAsync(W.iters.p, 0, sizeof(int) * chunk, G->stream));
-        CUDA_OR_RETURN(cudaMemsetAsync(W.flag.p, 1, chunk, G->stream));
-        // Every vector starts at zero, padding included: the stencil's bulk
-        // copies bring plane padding into the rows beyond the x2 edge, which
-        // must read as zero, and the kernels never write the padding.
-        CUDA_OR_RETURN(cudaMemsetAsync(W.x64.p, 0, sizeof(double) * vec, G->stream));
-        CUDA_OR_RETURN(cudaMemsetAsync(W.v0.p, 0, sizeof(T) * vec, G->stream));
-        CUDA_OR_RETURN(cudaMemsetAsync(W.v1.p, 0, sizeof(T) * vec, G->stream));
-        CUDA_OR_RETURN(cudaMemsetAsync(W.v2.p, 0, sizeof(T) * vec, G->stream));
-        if (mixed) CUDA_OR_RETURN(cudaMemsetAsync(W.v3.p, 0, sizeof(float) * vec, G->stream));
-        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
-
-        ColumnSet cs{};
-        cs.ncols = chunk;
-        cs.slip_node = W.slip_node.as<int>();
-        cs.slip_comp = W.slip_comp.as<int>();
-        cs.slip_dense = B.slip_dense ? W.slip_dense.as<double>() : nullptr;
-        cs.status = W.status.as<int8_t>();
-        const unsigned sb = (unsigned)((chunk + 127) / 128);
-        if (!generic) {
-            // r0 = b = H P (D+SAT) chi  (x = 0), in the working precision.
-            CUDA_OR_RETURN((launch_march<double, T, MODE_RHS>(G, W.x64.as<double>(), W.v0.as<T>(), cs,
-                                                               W.res_part.as<double>(), chunk)));
-            SolveParams sp2 = sp;
-            sp2.ntiles = nt64;
-            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), chunk, mixed);
-        } else {
-            // r0 = b given explicitly (reference layout, FP64).
-            CUDA_OR_RETURN(cudaMemcpyAsync(hbuf.p, B.rhs + (size_t)c0 * ntot, sizeof(double) * ntot * nc,
-                                           cudaMemcpyHostToDevice, G->stream));
-            const long long nel = ntot * nc;
-            ref_to_dev_kernel<double, T><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
-                hbuf.as<double>(), W.v0.as<T>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, nc);
-            // ||b||^2 through the update kernel's reduction with alpha = 0.
-            CUDA_OR_RETURN(cudaMemsetAsync(W.apply_part.p, 0, sizeof(double) * 2 * chunk * ntA, G->stream));
-            cg_update_kernel<T, double><<<(unsigned)(chunk * G->nchunks), 256, 0, G->stream>>>(
-                W.x64.as<double>(), W.v0.as<T>(), W.v1.as<T>(), W.v2.as<T>(), W.apply_part.as<double>(), st, sp,
-                W.rr_part.as<double>());
-            SolveParams sp2 = sp;
-            sp2.ntiles = G->nchunks;
-            // rr_part has stride 1; copy into the stride-2 layout the kernel reads.
-            CUDA_OR_RETURN(cudaMemsetAsync(W.res_part.p, 0, sizeof(double) * 2 * chunk * G->nchunks, G->stream));
-            CUDA_OR_RETURN(cudaMemcpy2DAsync(W.res_part.p, 2 * sizeof(double), W.rr_part.p, sizeof(double),
-                                             sizeof(double), (size_t)chunk * G->nchunks, cudaMemcpyDeviceToDevice,
-                                             G->stream));
-            cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), chunk, 0);
-        }
-        cg_pupdate_kernel<T><<<(unsigned)(chunk * G->nchunks), 256, 0, G->stream>>>(W.v1.as<T>(), W.v0.as<T>(), st, sp);
-        CUDA_OR_RETURN(cudaGetLastError());
-        launches += generic ? 4 : 3;
-
-        const long long itmax = o.itmax > 0 ? o.itmax : 2 * ntot;
-        long long launched = 0;
-        for (;;) {
-            count_active_kernel<<<1, 256, 0, G->stream>>>(W.status.as<int8_t>(), chunk, W.active.as<int>());
-            CUDA_OR_RETURN(cudaMemcpyAsync(W.h_active, W.active.p, sizeof(int), cudaMemcpyDeviceToHost, G->stream));
-            CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
-            if (*W.h_active == 0) break;
-            if (launched > itmax + kIter) break;
-            CUDA_OR_RETURN(cudaGraphLaunch(W.graph, G->stream));
-            launched += kIter;
-            launches += 1 + (int64_t)kIter * per_iter;
-        }
-        launches += 1;
-        rc = check_device_error(G);
+        rc = R.advance(done);
         if (rc) return rc;
-
-        // Outputs.
+        if (done.empty()) continue;
         if (!generic) {
-            ExtractGeom eg{gc.n1, gc.n2, gc.n3, gc.PS, gc.nf, gc.i2f0, gc.n2f, gc.i3f0, gc.n3f, gc.colstride, gc.mu};
-            const long long nthr = (long long)nc * gc.nf;
-            ColumnSet ce = cs;
-            ce.ncols = nc;
-            double *kdst = B.kdev ? B.kdev + (size_t)c0 * 2 * gc.nf : W.kout.as<double>();
-            extract_traction_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, G->stream>>>(
-                G->c64, eg, W.x64.as<double>(), ce, kdst, 2LL * gc.nf);
-            CUDA_OR_RETURN(cudaGetLastError());
-            launches += 1;
+            if (B.kdev) {
+                rc = R.extract(done, B.kdev, 2LL * gc.nf, true);
+            } else {
+                rc = R.extract(done, R.W->kout.template as<double>(), 2LL * gc.nf, false);
+                if (!rc && B.kcols)
+                    CUDA_OR_RETURN(cudaMemcpyAsync(kstage.data(), R.W->kout.p, sizeof(double) * 2 * gc.nf * done.size(),
+                                                   cudaMemcpyDeviceToHost, G->stream));
+            }
+            if (rc) return rc;
+        } else if (B.u_out) {
+            for (const ColDone &d : done) {
+                rc = R.solution(d.slot, B.u_out + (size_t)d.tag * ntot);
+                if (rc) return rc;
+            }
         }
-        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
-        if (!generic && B.kcols) {
-            CUDA_OR_RETURN(cudaMemcpyAsync(B.kcols + (size_t)c0 * 2 * gc.nf, W.kout.p, sizeof(double) * 2 * gc.nf * nc,
-                                           cudaMemcpyDeviceToHost, G->stream));
-        }
-        if (generic && B.u_out) {
-            const long long nel = ntot * nc;
-            dev_to_ref_kernel<double, double><<<(unsigned)((nel + tb - 1) / tb), tb, 0, G->stream>>>(
-                W.x64.as<double>(), hbuf.as<double>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, nc);
-            CUDA_OR_RETURN(cudaMemcpyAsync(B.u_out + (size_t)c0 * ntot, hbuf.p, sizeof(double) * ntot * nc,
-                                           cudaMemcpyDeviceToHost, G->stream));
-        }
-        CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), W.iters.p, sizeof(int) * chunk, cudaMemcpyDeviceToHost, G->stream));
-        CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), W.status.p, chunk, cudaMemcpyDeviceToHost, G->stream));
         CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, G->ev0, G->ev1);
-        dev_ms_total += ms;
-        for (int i = 0; i < nc; ++i) {
-            tot_it += hit[i];
-            max_it = std::max<int64_t>(max_it, hit[i]);
-            if (hst[i] != COL_CONVERGED) ++unconv;
-            if (B.iters) B.iters[c0 + i] = hit[i];
-            if (B.status) B.status[c0 + i] = hst[i] == COL_ACTIVE ? (int8_t)EQD_COL_MAXITER : hst[i];
+        for (size_t j = 0; j < done.size(); ++j) {
+            const ColDone &d = done[j];
+            if (!generic && B.kcols && !B.kdev)
+                std::memcpy(B.kcols + (size_t)d.tag * 2 * gc.nf, kstage.data() + j * 2 * gc.nf,
+                            sizeof(double) * 2 * gc.nf);
+            tot_it += d.iters;
+            max_it = std::max<int64_t>(max_it, d.iters);
+            if (d.status != COL_CONVERGED) ++unconv;
+            if (B.iters) B.iters[d.tag] = d.iters;
+            if (B.status) B.status[d.tag] = d.status;
         }
+        finished += (int)done.size();
+        rc = R.release(done);
+        if (rc) return rc;
     }
+    CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+    CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, G->ev0, G->ev1);
     if (stats) {
         stats->solves += B.ncols;
         stats->iterations += tot_it;
         stats->max_iterations = std::max<int64_t>(stats->max_iterations, max_it);
         stats->unconverged += unconv;
-        stats->reliable_updates += reliable;
-        stats->kernel_launches += launches;
-        stats->device_seconds += dev_ms_total * 1e-3;
+        stats->kernel_launches += R.launches;
+        stats->device_seconds += ms * 1e-3;
         stats->precision = o.precision;
         stats->precond = o.precond;
     }

@@ -74,13 +74,15 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
     if (threadIdx.x == 0) rr_part[(long long)col * sp.nchunks + chunk] = s;
 }
 
-// p = r + beta p for active columns.
+// p = r + beta p for active columns (only the masked ones when `mask` is set:
+// the first direction of columns that just entered the batch).
 template <typename T>
 __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, const T *__restrict__ r, ColState st,
-                                                         SolveParams sp) {
+                                                         SolveParams sp, const int8_t *__restrict__ mask = nullptr) {
     const int col = blockIdx.x / sp.nchunks;
     const int chunk = blockIdx.x % sp.nchunks;
     if (st.status[col] != COL_ACTIVE) return;
+    if (mask && !mask[col]) return;
     const T b = (T)st.beta[col];
     const long long n = sp.colstride;
     const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
@@ -156,11 +158,13 @@ __global__ void cg_scalar_kernel(ColState st, SolveParams sp, const double *__re
 
 // After a true-residual evaluation (start of a solve, or a reliable update).
 // `first`: this is r0 = b (sets ||b|| and the tolerance).
+// `mask` (optional) restricts the kernel to the columns that just entered the
+// batch (their r0 = b evaluation).
 __global__ void cg_true_residual_kernel(ColState st, SolveParams sp, const double *__restrict__ res_part, int ncols,
-                                        int mixed) {
+                                        int mixed, const int8_t *__restrict__ mask = nullptr) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncols || st.status[col] != COL_ACTIVE) return;
-    if (mixed && !st.flag[col]) return;
+    if (mask ? !mask[col] : (mixed && !st.flag[col])) return;
     const double rr = sum_parts(res_part, col, sp.ntiles, 2, 0);
     const int it = st.iters[col];
     if (it == 0) {
@@ -188,6 +192,39 @@ __global__ void cg_true_residual_kernel(ColState st, SolveParams sp, const doubl
         st.beta[col] = rr / st.gamma[col];
         st.gamma[col] = rr;
         st.rr_ref[col] = rr;
+    }
+}
+
+// Zero the vectors of the masked columns (padding included: the stencil's
+// bulk copies read plane padding, which must stay zero).
+template <typename T>
+__global__ void __launch_bounds__(256) zero_columns_kernel(T *__restrict__ v, long long colstride, int nchunks,
+                                                           const int8_t *__restrict__ mask) {
+    const int col = blockIdx.x / nchunks;
+    const int chunk = blockIdx.x % nchunks;
+    if (!mask[col]) return;
+    const long long beg = colstride * chunk / nchunks, end = colstride * (chunk + 1) / nchunks;
+    T *vc = v + (long long)col * colstride;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) vc[i] = T(0);
+}
+
+// Per-column sum of squares of the masked columns, partials laid out as the
+// stencil's [column][chunk][2] (slot 0) so cg_true_residual_kernel reads them.
+template <typename T>
+__global__ void __launch_bounds__(256) column_sumsq_kernel(const T *__restrict__ v, long long colstride, int nchunks,
+                                                           const int8_t *__restrict__ mask, double *__restrict__ part) {
+    const int col = blockIdx.x / nchunks;
+    const int chunk = blockIdx.x % nchunks;
+    if (!mask[col]) return;
+    __shared__ double red[32];
+    const long long beg = colstride * chunk / nchunks, end = colstride * (chunk + 1) / nchunks;
+    const T *vc = v + (long long)col * colstride;
+    double acc = 0.0;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) acc += (double)vc[i] * (double)vc[i];
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        part[((long long)col * nchunks + chunk) * 2 + 0] = s;
+        part[((long long)col * nchunks + chunk) * 2 + 1] = 0.0;
     }
 }
 
@@ -232,13 +269,18 @@ __device__ __forceinline__ double d1_row(const AxisT<double> &a, int n, int r, F
     return s;
 }
 
+// Entry j of the list extracts column slot slots[j] (j itself without a list)
+// into K column dstcol[j] (j without a map), leading dimension kld.
 __global__ void extract_traction_kernel(const __grid_constant__ OpConst<double> C, ExtractGeom g,
                                         const double *__restrict__ x, ColumnSet cs, double *__restrict__ K,
-                                        long long kld) {
+                                        long long kld, int nlist, const int *__restrict__ slots,
+                                        const int *__restrict__ dstcol) {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int col = (int)(gid / g.nf);
+    const int j = (int)(gid / g.nf);
     const int k = (int)(gid % g.nf);
-    if (col >= cs.ncols) return;
+    if (j >= nlist) return;
+    const int col = slots ? slots[j] : j;
+    const long long kc = dstcol ? dstcol[j] : j;
     const int a = k % g.n2f, b = k / g.n2f;
     const int i2 = g.i2f0 + a, i3 = g.i3f0 + b;
     const int n1 = g.n1, n2 = g.n2, n3 = g.n3;
@@ -282,8 +324,8 @@ __global__ void extract_traction_kernel(const __grid_constant__ OpConst<double> 
         }
         dt[j] = 0.5 * t;
     }
-    K[(long long)col * kld + k] = dt[0];
-    K[(long long)col * kld + g.nf + k] = dt[1];
+    K[kc * kld + k] = dt[0];
+    K[kc * kld + g.nf + k] = dt[1];
 }
 
 // ---------------------------------------------------------------------------
