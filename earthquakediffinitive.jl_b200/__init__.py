@@ -41,7 +41,7 @@ __all__ = [
     "CGStats", "split_node_solve", "solver_report", "merge_stats", "duplicate",
     "elastic_solver_report", "frictional_node_count", "fault_grid_axes", "shear_traction",
     "fault_stiffness", "fault_stiffness_toeplitz", "stiffness_columns", "apply_operator",
-    "KMatrix", "build_model", "EqdError", "EqdArgumentError", "library_path",
+    "KMatrix", "build_model", "EqdError", "EqdArgumentError", "library_path", "Server",
 ]
 
 
@@ -423,3 +423,6 @@ def build_model(dz=50.0, L_fault=800.0, L_normal=400.0, l_f=400.0, mu=32.04e9, n
     info = dict(dz=dz, L_fault=L_fault, L_normal=L_normal, n1=g.n1, n23=g.n2, order=4,
                 elastic_dofs=g.ntot, n2f=fe.n2f, n3f=fe.n3f)
     return dict(fe=fe, K=K, nf=fe.nf, x2=fe.x2f.copy(), x3=fe.x3f.copy(), grid_info=info)
+
+
+from .serving import Server  # noqa: E402  (continuous-batching request server)

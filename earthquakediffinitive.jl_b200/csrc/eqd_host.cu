@@ -9,7 +9,11 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <condition_variable>
+#include <deque>
+#include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/eqd.h"
@@ -71,6 +75,7 @@ static constexpr int kMaxT32 = 640;   // generic FP32 instances
 static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register spills
 static constexpr int kMaxT32c = 384;  // FP32 A-apply, two columns per thread
 static constexpr int kMaxT64 = 384;
+static constexpr int kMaxT64b = 512;  // FP64 instances for wide x1 lines (n1 = 33 needs 7 x 66 threads)
 static constexpr int kNumVariants = 5;
 
 static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
@@ -91,8 +96,18 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     // Balanced tiles, every tile at least 7 rows: the wide operator's closure
     // rows reach 10 rows in from the boundary, and a tile reads 4 halo rows.
     while (ntiles > 1 && n2 / ntiles < 7) --ntiles;
-    const int t2max = (n2 + ntiles - 1) / ntiles;
-    if (t2max * per_row > maxt || n2 / ntiles < std::min(7, n2)) {
+    int t2max = (n2 + ntiles - 1) / ntiles;
+    int edge = 0;
+    if (t2max * per_row > maxt && t2 >= 7 && n2 >= 14) {
+        // Tiles of at most t2 rows: 7-row tiles at both ends carry the closure
+        // rows, the tiles between (any height) split the interior.
+        edge = 7;
+        const int m = n2 - 2 * edge;
+        const int nm = m > 0 ? (m + t2 - 1) / t2 : 0;
+        ntiles = nm + 2;
+        t2max = std::max(edge, nm > 0 ? (m + nm - 1) / nm : 0);
+    }
+    if (t2max * per_row > maxt || (edge == 0 && n2 / ntiles < std::min(7, n2))) {
         why = "grid too large in x1 for one CTA (n1=" + std::to_string(n1) + ")";
         return false;
     }
@@ -115,6 +130,7 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     out.g.colstride = colstride;
     out.g.ntiles = ntiles;
     out.g.t2max = t2max;
+    out.g.edge = edge;
     out.g.CH = CH;
     out.g.i2f0 = gc.i2f0;
     out.g.n2f = gc.n2f;
@@ -165,6 +181,8 @@ struct eqd_grid {
     OpConst<float> c32;
     OpConst<double> c64;
     MarchCfg m32, m64;
+    int m64_maxt = 384;   // launch bound of the FP64 instance the grid runs
+    bool served = false;  // attached to an eqd_server (its worker owns the grid)
     // FP32 A-apply launch variants (see make_variants) and the chosen one.
     MarchCfg v32[kNumVariants];
     int v32_maxt[kNumVariants] = {};
@@ -241,9 +259,16 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
     const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
                                                                                : (const void *)&G->c64);
     dim3 grid((unsigned)(ncols * m.g.ntiles));
+    const bool wide64 = sizeof(T) == 8 && G->m64_maxt == kMaxT64b;
     if (MODE == MODE_AP) {  // generic-input hook: runtime-n1 instance only
-        plane_march_kernel<T, TO, MODE, MAXT, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
-            C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+        if (wide64)
+            plane_march_kernel<T, TO, MODE, kMaxT64b, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
+                C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+        else
+            plane_march_kernel<T, TO, MODE, MAXT, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
+                C, m.g, in, out, cs, partials, G->err.as<unsigned>());
+    } else if (wide64) {
+        launch_n1<T, TO, MODE, kMaxT64b>(n1, grid, m, G->stream, C, in, out, cs, partials, G->err.as<unsigned>());
     } else {
         launch_n1<T, TO, MODE, MAXT>(n1, grid, m, G->stream, C, in, out, cs, partials, G->err.as<unsigned>());
     }
@@ -259,11 +284,15 @@ static cudaError_t configure_kernels(int smem_max) {
         (const void *)plane_march_kernel<float, float, MODE_RHS, kMaxT32, N, 1>,   \
         (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64, N, 1>,   \
         (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64, N, 1>, \
-        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64, N, 1>,
+        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64, N, 1>,   \
+        (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64b, N, 1>,  \
+        (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64b, N, 1>, \
+        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64b, N, 1>,
     const void *ks[] = {
         EQD_FOR_N1(EQD_KS) EQD_KS(0)
         (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32, 0, 1>,
         (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64, 0, 1>,
+        (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64b, 0, 1>,
     };
 #undef EQD_KS
     for (const void *k : ks) {
@@ -379,9 +408,15 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     fill_op<float>(G->c32, gc, G->h);
     fill_op<double>(G->c64, gc, G->h);
     std::string why;
-    if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT32, 0, gc, G->m32, why) ||
-        !make_march_cfg<double>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT64, 0, gc, G->m64, why))
+    if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT32, 0, gc, G->m32, why))
         return fail(EQD_ERR_ARG, why);
+    // FP64: the 384-thread instance where a tile fits, else the 512-thread one.
+    G->m64_maxt = kMaxT64;
+    if (!make_march_cfg<double>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT64, 0, gc, G->m64, why)) {
+        G->m64_maxt = kMaxT64b;
+        if (!make_march_cfg<double>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, kMaxT64b, 0, gc, G->m64, why))
+            return fail(EQD_ERR_ARG, why);
+    }
     // FP32 A-apply variants: one large CTA per SM (640-thread bound, may
     // spill), one CTA of up to 512 threads (no spill), and CTAs of up to 256
     // threads so that two share an SM.
@@ -427,6 +462,10 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
 
 extern "C" int eqd_grid_destroy(eqd_grid *G) {
     if (!G) return EQD_OK;
+    {
+        std::lock_guard<std::mutex> lk(G->mtx);
+        if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server; destroy the server first");
+    }
     cudaSetDevice(G->desc.device);
     if (G->stream) cudaStreamSynchronize(G->stream);
     if (G->ev0) cudaEventDestroy(G->ev0);
@@ -503,6 +542,7 @@ extern "C" int eqd_apply(eqd_grid *G, const double *x, double *y, int32_t ncols,
     if (ncols < 1) return fail(EQD_ERR_ARG, "ncols must be >= 1");
     if (mode < 0 || mode > 2) return fail(EQD_ERR_ARG, "mode must be 0 (A), 1 (HP_DSAT) or 2 (A, input in range(P))");
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     if (precision == EQD_PREC_FP64) return apply_impl<double>(G, x, y, ncols, mode);
     if (precision == EQD_PREC_MIXED) return apply_impl<float>(G, x, y, ncols, mode);
@@ -650,6 +690,34 @@ struct ColDone {
     int8_t status;
 };
 
+// Page-locked host array: device-to-host copies into it stay asynchronous.
+template <typename E>
+struct PinnedArr {
+    E *p = nullptr;
+    int n = 0;
+    PinnedArr() = default;
+    PinnedArr(const PinnedArr &) = delete;
+    PinnedArr &operator=(const PinnedArr &) = delete;
+    ~PinnedArr() {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t assign(int count, E v) {
+        if (count > n) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            n = 0;
+            cudaError_t e = cudaHostAlloc((void **)&p, sizeof(E) * std::max(count, 1), cudaHostAllocDefault);
+            if (e != cudaSuccess) return e;
+            n = count;
+        }
+        for (int i = 0; i < count; ++i) p[i] = v;
+        return cudaSuccess;
+    }
+    E *data() { return p; }
+    E &operator[](int i) { return p[i]; }
+    const E &operator[](int i) const { return p[i]; }
+};
+
 template <typename T>
 struct SlotRun {
     eqd_grid *G = nullptr;
@@ -658,8 +726,10 @@ struct SlotRun {
     long long itmax = 0;
     SolveParams sp{};
     ColState st{};
-    std::vector<int> hn, hc, hit, hslot, hdst;
-    std::vector<int8_t> hst, hnew;
+    std::vector<int> hn, hc, hslot, hdst;
+    std::vector<int8_t> hnew;
+    PinnedArr<int> hit;     // per-slot iteration counts (read back every graph launch)
+    PinnedArr<int8_t> hst;  // per-slot status
     std::vector<long long> tag;  // -1: free slot
     int held = 0;                // occupied slots (running or finished, not yet released)
     int64_t launches = 0;
@@ -722,8 +792,8 @@ struct SlotRun {
         // columns enter.
         hn.assign(cap, -1);
         hc.assign(cap, 0);
-        hit.assign(cap, 0);
-        hst.assign(cap, (int8_t)COL_IDLE);
+        CUDA_OR_RETURN(hit.assign(cap, 0));
+        CUDA_OR_RETURN(hst.assign(cap, (int8_t)COL_IDLE));
         hnew.assign(cap, 0);
         tag.assign(cap, -1);
         hslot.resize(cap);
@@ -846,10 +916,10 @@ struct SlotRun {
         return EQD_OK;
     }
 
-    // Run kIter iterations (when a column is running), then list the occupied
-    // slots whose status is final.
-    int advance(std::vector<ColDone> &done) {
-        done.clear();
+    // Run kIter iterations (when a column is running) and queue the status
+    // read-back; collect() then lists the finished slots. Split in two so that
+    // a caller driving several grids can have all of them running at once.
+    int launch() {
         Workspace &w = *W;
         int running = 0;
         for (int s = 0; s < cap; ++s) running += tag[s] >= 0 && hst[s] == COL_ACTIVE;
@@ -859,6 +929,19 @@ struct SlotRun {
         }
         CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), w.status.p, cap, cudaMemcpyDeviceToHost, G->stream));
         CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), w.iters.p, sizeof(int) * cap, cudaMemcpyDeviceToHost, G->stream));
+        return EQD_OK;
+    }
+
+    int advance(std::vector<ColDone> &done) {
+        int rc = launch();
+        return rc ? rc : collect(done);
+    }
+
+    // Wait for the queued iterations; list the occupied slots whose status is
+    // final.
+    int collect(std::vector<ColDone> &done) {
+        done.clear();
+        Workspace &w = *W;
         CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
         int rc = check_device_error(G);
         if (rc) return rc;
@@ -1030,6 +1113,7 @@ static int run_batch_any(eqd_grid *G, const eqd_solve_opts *opts, const BatchSpe
     if (B.rhs && o.precision != EQD_PREC_FP64) return fail(EQD_ERR_UNSUPPORTED, "explicit-RHS solves run in FP64");
     const auto t0 = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     int rc = o.precision == EQD_PREC_MIXED ? run_batch<float>(G, o, B, stats) : run_batch<double>(G, o, B, stats);
     if (stats)
@@ -1159,6 +1243,7 @@ extern "C" int eqd_stiffness_toeplitz(eqd_grid *G, const eqd_solve_opts *opts, d
     int rc = eqd_stiffness_columns(G, cols.data(), 10, opts, resp.data(), nullptr, nullptr, stats);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     const size_t N = 2 * (size_t)nf;
     DevBuf dK, dsrc, da, db;
@@ -1213,6 +1298,7 @@ extern "C" int eqd_profile_apply(eqd_grid *G, int32_t ncols, int32_t precision, 
                                  double *ms_per_launch, double *bytes_per_launch) {
     if (!G || ncols < 1 || reps < 1 || warmup < 0) return fail(EQD_ERR_ARG, "invalid argument");
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     if (precision == EQD_PREC_MIXED) return profile_apply_impl<float>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
     if (precision == EQD_PREC_FP64) return profile_apply_impl<double>(G, ncols, warmup, reps, ms_per_launch, bytes_per_launch);
@@ -1223,6 +1309,7 @@ extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, doubl
                             int32_t *tile_rows, int32_t *threads, int32_t *nvariants) {
     if (!G || ncols < 1) return fail(EQD_ERR_ARG, "invalid argument");
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     int rc = tune_variants(G, ncols);
     if (rc) return rc;
@@ -1239,6 +1326,7 @@ extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, doubl
 extern "C" int eqd_set_variant(eqd_grid *G, int32_t variant) {
     if (!G || variant < 0 || variant >= kNumVariants) return fail(EQD_ERR_ARG, "invalid variant");
     std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     G->sel32 = variant;
     G->tuned = true;
     return EQD_OK;
@@ -1372,5 +1460,368 @@ extern "C" int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_d
     cudaError_t e = cudaGetLastError();
     if (prev != device) cudaSetDevice(prev);
     if (e != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("eqd_kmat_gemv_static launch: ") + cudaGetErrorString(e));
+    return EQD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Server: continuous batching of stiffness-column requests across grids.
+// One worker thread drives every attached grid's slot engine: it admits
+// queued columns into free slots, starts each grid's next graph of
+// iterations (grids on their own streams, so their work overlaps on the
+// device), then collects finished columns and writes them to their
+// requests' host buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SrvRequest {
+    int64_t id = 0;
+    double *k_out = nullptr;
+    int ncols = 0, remaining = 0, unconverged = 0, max_it = 0;
+    int64_t iterations = 0;
+    int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
+    int err = EQD_OK;
+    std::string msg;
+    double t_submit = 0, t_start = -1, t_done = -1;
+};
+
+struct SrvGrid {
+    eqd_grid *G = nullptr;
+    int slots = 0;
+    size_t bytes = 0;
+    std::unique_ptr<SlotRun<float>> r32;
+    std::unique_ptr<SlotRun<double>> r64;
+    std::deque<ColWork> pending;  // guarded by the server mutex
+    PinnedArr<double> kstage;     // finished K columns, compact
+    std::vector<ColDone> done;
+    bool launched = false;
+    int held() const { return r32 ? r32->held : r64->held; }
+    int free_slots() const { return r32 ? r32->free_slots() : r64->free_slots(); }
+};
+
+// Column tags carry the request id and the column's position in it.
+constexpr int kTagBits = 24;
+
+}  // namespace
+
+struct eqd_server {
+    eqd_solve_opts opts{};
+    uint64_t budget = 0, used = 0;
+    std::vector<std::unique_ptr<SrvGrid>> grids;
+    std::map<int64_t, std::unique_ptr<SrvRequest>> reqs;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false, started = false;
+    int64_t next_id = 1;
+    int fatal = EQD_OK;
+    std::string fatal_msg;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+static void server_fail_all(eqd_server *S, int code, const std::string &msg) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->fatal = code;
+    S->fatal_msg = msg;
+    for (auto &kv : S->reqs) {
+        SrvRequest &r = *kv.second;
+        if (r.state < 2) {
+            r.state = 3;
+            r.err = code;
+            r.msg = msg;
+            r.t_done = S->now();
+        }
+    }
+    for (auto &g : S->grids) g->pending.clear();
+    S->cv_done.notify_all();
+}
+
+// One pass of the worker over every grid. Returns an error code.
+static int server_pass(eqd_server *S) {
+    // Phase 1: admit queued columns and start each busy grid's iterations.
+    for (auto &gp : S->grids) {
+        SrvGrid &g = *gp;
+        g.launched = false;
+        std::vector<ColWork> take;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            const int nfree = g.free_slots();
+            while ((int)take.size() < nfree && !g.pending.empty()) {
+                take.push_back(g.pending.front());
+                g.pending.pop_front();
+            }
+            const double t = S->now();
+            for (const ColWork &c : take) {
+                auto it = S->reqs.find(c.tag >> kTagBits);
+                if (it != S->reqs.end() && it->second->state == 0) {
+                    it->second->state = 1;
+                    it->second->t_start = t;
+                }
+            }
+        }
+        if (cudaSetDevice(g.G->desc.device) != cudaSuccess) return fail(EQD_ERR_CUDA, "cudaSetDevice failed");
+        int rc = EQD_OK, taken = 0;
+        if (!take.empty())
+            rc = g.r32 ? g.r32->admit(take.data(), (int)take.size(), taken)
+                       : g.r64->admit(take.data(), (int)take.size(), taken);
+        if (rc) return rc;
+        if (g.held() > 0) {
+            rc = g.r32 ? g.r32->launch() : g.r64->launch();
+            if (rc) return rc;
+            g.launched = true;
+        }
+    }
+    // Phase 2: collect finished columns, extract their K columns, deliver.
+    for (auto &gp : S->grids) {
+        SrvGrid &g = *gp;
+        if (!g.launched) continue;
+        eqd_grid *G = g.G;
+        if (cudaSetDevice(G->desc.device) != cudaSuccess) return fail(EQD_ERR_CUDA, "cudaSetDevice failed");
+        int rc = g.r32 ? g.r32->collect(g.done) : g.r64->collect(g.done);
+        if (rc) return rc;
+        if (g.done.empty()) continue;
+        const int nf2 = 2 * G->gc.nf;
+        rc = g.r32 ? g.r32->extract(g.done, G->ws.kout.as<double>(), nf2, false)
+                   : g.r64->extract(g.done, G->ws.kout.as<double>(), nf2, false);
+        if (rc) return rc;
+        CUDA_OR_RETURN(cudaMemcpyAsync(g.kstage.data(), G->ws.kout.p, sizeof(double) * nf2 * g.done.size(),
+                                       cudaMemcpyDeviceToHost, G->stream));
+        CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            const double t = S->now();
+            bool any_done = false;
+            for (size_t j = 0; j < g.done.size(); ++j) {
+                const ColDone &d = g.done[j];
+                auto it = S->reqs.find(d.tag >> kTagBits);
+                if (it == S->reqs.end()) continue;
+                SrvRequest &r = *it->second;
+                const long long pos = d.tag & ((1LL << kTagBits) - 1);
+                std::memcpy(r.k_out + (size_t)pos * nf2, g.kstage.data() + j * nf2, sizeof(double) * nf2);
+                r.iterations += d.iters;
+                r.max_it = std::max(r.max_it, d.iters);
+                if (d.status != COL_CONVERGED) ++r.unconverged;
+                if (--r.remaining == 0) {
+                    r.state = 2;
+                    r.t_done = t;
+                    any_done = true;
+                }
+            }
+            if (any_done) S->cv_done.notify_all();
+        }
+        rc = g.r32 ? g.r32->release(g.done) : g.r64->release(g.done);
+        if (rc) return rc;
+    }
+    return EQD_OK;
+}
+
+static void server_loop(eqd_server *S) {
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_work.wait(lk, [&] {
+                if (S->stop) return true;
+                for (auto &g : S->grids)
+                    if (!g->pending.empty() || g->held() > 0) return true;
+                return false;
+            });
+            if (S->stop) return;
+        }
+        const int rc = server_pass(S);
+        if (rc) {
+            server_fail_all(S, rc, g_last_error);
+            return;
+        }
+    }
+}
+
+extern "C" int eqd_server_create(const eqd_solve_opts *opts, uint64_t hbm_budget_bytes, eqd_server **out) {
+    if (!out) return fail(EQD_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::unique_ptr<eqd_server> S(new eqd_server());
+    if (opts) S->opts = *opts;
+    else eqd_default_opts(&S->opts);
+    const eqd_solve_opts &o = S->opts;
+    if (!(o.rtol >= 0) || !(o.atol >= 0)) return fail(EQD_ERR_ARG, "rtol/atol must be non-negative");
+    if (o.precision != EQD_PREC_FP64 && o.precision != EQD_PREC_MIXED) return fail(EQD_ERR_ARG, "unknown precision");
+    if (o.precond == EQD_PRECOND_JACOBI)
+        return fail(EQD_ERR_UNSUPPORTED, "precond=:jacobi is not available on this path");
+    if (o.precond != EQD_PRECOND_NONE) return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
+    S->budget = hbm_budget_bytes;
+    if (S->budget == 0) {
+        size_t fr = 0, tot = 0;
+        CUDA_OR_RETURN(cudaMemGetInfo(&fr, &tot));
+        const size_t keep = (size_t)2 << 30;
+        S->budget = fr > keep ? fr - keep : fr / 2;
+    }
+    *out = S.release();
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_add_grid(eqd_server *S, eqd_grid *G, int32_t slots) {
+    if (!S || !G || slots < 0) return fail(EQD_ERR_ARG, "invalid argument");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (auto &g : S->grids)
+            if (g->G == G) return fail(EQD_ERR_ARG, "grid already attached");
+    }
+    std::lock_guard<std::mutex> glk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to another server");
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    const GridConst &gc = G->gc;
+    const int mixed = S->opts.precision == EQD_PREC_MIXED;
+    const size_t per_slot = (size_t)gc.colstride * (mixed ? (8 + 4 * 4) : (8 + 3 * 8)) + (size_t)16 * gc.nf + 1024;
+    std::unique_ptr<SrvGrid> g(new SrvGrid());
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        const uint64_t left = S->budget > S->used ? S->budget - S->used : 0;
+        const long long fit = (long long)(left / per_slot);
+        const int want = slots > 0 ? slots : (int)std::min<long long>(fit, 512);
+        if (want < 1 || (long long)want > fit)
+            return fail(EQD_ERR_OOM, "the server's HBM budget has room for " + std::to_string(fit) +
+                                         " slot(s) of this grid");
+        g->slots = want;
+        g->bytes = (size_t)want * per_slot;
+        S->used += g->bytes;
+    }
+    g->G = G;
+    int rc;
+    if (mixed) {
+        g->r32.reset(new SlotRun<float>());
+        rc = g->r32->setup(G, S->opts, g->slots, false, false);
+    } else {
+        g->r64.reset(new SlotRun<double>());
+        rc = g->r64->setup(G, S->opts, g->slots, false, false);
+    }
+    if (!rc) {
+        cudaError_t e = g->kstage.assign(2 * gc.nf * g->slots, 0.0);
+        if (e != cudaSuccess) rc = fail(EQD_ERR_OOM, "pinned staging buffer");
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(G->stream);
+        if (e != cudaSuccess) rc = fail(EQD_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->used -= g->bytes;
+        return rc;
+    }
+    G->served = true;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->grids.push_back(std::move(g));
+    if (!S->started) {
+        S->started = true;
+        S->worker = std::thread(server_loop, S);
+    }
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_submit(eqd_server *S, eqd_grid *G, const int32_t *cols, int32_t ncols, double *k_out,
+                                 int64_t *request_id) {
+    if (!S || !G || (!cols && ncols > 0) || ncols < 0 || (!k_out && ncols > 0) || !request_id)
+        return fail(EQD_ERR_ARG, "invalid argument");
+    if (ncols >= (1 << kTagBits)) return fail(EQD_ERR_ARG, "too many columns in one request");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->fatal) return fail(S->fatal, "server stopped: " + S->fatal_msg);
+    SrvGrid *g = nullptr;
+    for (auto &x : S->grids)
+        if (x->G == G) g = x.get();
+    if (!g) return fail(EQD_ERR_ARG, "grid not attached to this server");
+    const int nf = G->gc.nf;
+    for (int i = 0; i < ncols; ++i)
+        if (cols[i] < 0 || cols[i] >= 2 * nf) return fail(EQD_ERR_ARG, "column index out of range");
+    std::unique_ptr<SrvRequest> r(new SrvRequest());
+    r->id = S->next_id++;
+    r->k_out = k_out;
+    r->ncols = r->remaining = ncols;
+    r->t_submit = S->now();
+    if (ncols == 0) {
+        r->state = 2;
+        r->t_start = r->t_done = r->t_submit;
+    }
+    for (int i = 0; i < ncols; ++i) {
+        ColWork c;
+        c.slip_node = cols[i] % nf;
+        c.slip_comp = cols[i] / nf;
+        c.tag = (r->id << kTagBits) | i;
+        g->pending.push_back(c);
+    }
+    *request_id = r->id;
+    S->reqs[r->id] = std::move(r);
+    S->cv_work.notify_one();
+    return EQD_OK;
+}
+
+static SrvRequest *find_req(eqd_server *S, int64_t id) {
+    auto it = S->reqs.find(id);
+    return it == S->reqs.end() ? nullptr : it->second.get();
+}
+
+extern "C" int eqd_server_wait(eqd_server *S, int64_t id, double timeout_s) {
+    if (!S) return fail(EQD_ERR_ARG, "null server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    SrvRequest *r = find_req(S, id);
+    if (!r) return fail(EQD_ERR_ARG, "unknown request id");
+    const auto pred = [&] { return r->state >= 2; };
+    if (timeout_s < 0) S->cv_done.wait(lk, pred);
+    else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred))
+        return fail(EQD_ERR_TIMEOUT, "request not done within the timeout");
+    if (r->state == 3) return fail(r->err, r->msg);
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_poll(eqd_server *S, int64_t id, int32_t *done) {
+    if (!S || !done) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    SrvRequest *r = find_req(S, id);
+    if (!r) return fail(EQD_ERR_ARG, "unknown request id");
+    *done = r->state >= 2;
+    if (r->state == 3) return fail(r->err, r->msg);
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_request_info(eqd_server *S, int64_t id, eqd_request_info *info) {
+    if (!S || !info) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    SrvRequest *r = find_req(S, id);
+    if (!r) return fail(EQD_ERR_ARG, "unknown request id");
+    info->state = r->state;
+    info->ncols = r->ncols;
+    info->unconverged = r->unconverged;
+    info->max_iterations = r->max_it;
+    info->iterations = r->iterations;
+    info->t_submit = r->t_submit;
+    info->t_start = r->t_start;
+    info->t_done = r->t_done;
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_release(eqd_server *S, int64_t id) {
+    if (!S) return fail(EQD_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    SrvRequest *r = find_req(S, id);
+    if (!r) return fail(EQD_ERR_ARG, "unknown request id");
+    if (r->state < 2) return fail(EQD_ERR_ARG, "request still in flight");
+    S->reqs.erase(id);
+    return EQD_OK;
+}
+
+extern "C" int eqd_server_destroy(eqd_server *S) {
+    if (!S) return EQD_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    if (S->worker.joinable()) S->worker.join();
+    for (auto &g : S->grids) {
+        cudaSetDevice(g->G->desc.device);
+        cudaStreamSynchronize(g->G->stream);
+        g->r32.reset();
+        g->r64.reset();
+        std::lock_guard<std::mutex> glk(g->G->mtx);
+        g->G->served = false;
+    }
+    delete S;
     return EQD_OK;
 }

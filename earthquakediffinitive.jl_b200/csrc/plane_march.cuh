@@ -88,6 +88,8 @@ struct MarchGeom {
     long long colstride;
     int ntiles;            // x2 tiles per column
     int t2max;             // rows per tile (upper bound)
+    int edge;              // > 0: the first and last tiles have `edge` rows and the
+                           // tiles between split the rest evenly; 0: all balanced
     int CH;                // ring chunk capacity (elements) per (side, comp)
     int i2f0, n2f, i3f0, n3f, nf;
 };
@@ -275,8 +277,25 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
     const int n1 = N1 > 0 ? N1 : g.n1;
     const int n2 = g.n2, n3 = g.n3;
-    const int a0 = (int)((long long)tile * n2 / g.ntiles);
-    const int a1 = (int)((long long)(tile + 1) * n2 / g.ntiles);
+    int a0, a1;
+    if (g.edge > 0) {
+        // Edge tiles hold every closure row (and read the 11 rows the wide
+        // operator's closures reach); the middle tiles only need the halo.
+        if (tile == 0) {
+            a0 = 0;
+            a1 = g.edge;
+        } else if (tile == g.ntiles - 1) {
+            a0 = n2 - g.edge;
+            a1 = n2;
+        } else {
+            const int m = n2 - 2 * g.edge, nm = g.ntiles - 2, k = tile - 1;
+            a0 = g.edge + (int)((long long)k * m / nm);
+            a1 = g.edge + (int)((long long)(k + 1) * m / nm);
+        }
+    } else {
+        a0 = (int)((long long)tile * n2 / g.ntiles);
+        a1 = (int)((long long)(tile + 1) * n2 / g.ntiles);
+    }
     constexpr int AE = 16 / (int)sizeof(T);  // elements per 16 bytes
 
     // Row range copied per plane (tile + halo, clipped), 16-byte aligned.

@@ -207,6 +207,49 @@ int eqd_kmat_destroy(eqd_kmat *kmat);
 int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_device, const double *s_device,
                          double *y_device, int32_t nvec, void *stream);
 
+/* Serving: stiffness-column requests answered by continuous batching -------
+ * The reference builds K in one blocking call (`fault_stiffness`,
+ * src/FaultResponse.jl:229-287, its column loop `run_columns!` :244-263).
+ * The server answers requests for subsets of K's columns on several grids as
+ * they arrive: each attached grid keeps a pool of CG slots (operator tables,
+ * Krylov vectors and per-column state resident in HBM); a request's columns
+ * enter free slots as earlier columns finish, beside the columns of other
+ * requests on the same grid; grids run concurrently on their own streams.
+ * A column's result does not depend on what else is in flight. */
+typedef struct {
+    int32_t state;            /* 0 queued, 1 running, 2 done, 3 failed */
+    int32_t ncols;
+    int32_t unconverged;
+    int32_t max_iterations;
+    int64_t iterations;       /* sum over the request's columns */
+    double t_submit;          /* seconds on the server clock */
+    double t_start;           /* first column entered a slot */
+    double t_done;            /* last column extracted */
+} eqd_request_info;
+
+/* `opts` fixes the solver for every grid (NULL: defaults); the slot pools of
+ * all grids together stay within `hbm_budget_bytes` (0: free memory - 2 GiB). */
+int eqd_server_create(const eqd_solve_opts *opts, uint64_t hbm_budget_bytes, eqd_server **out);
+/* Attach a grid with `slots` CG slots (0: as many as the remaining budget
+ * allows, at most 512). The grid then belongs to the server until
+ * eqd_server_destroy: other calls on it fail with EQD_ERR_ARG. */
+int eqd_server_add_grid(eqd_server *server, eqd_grid *grid, int32_t slots);
+/* Queue K columns `cols` (0-based, < 2nf) of an attached grid; the result,
+ * 2nf x ncols column-major FP64, goes to the caller-owned host buffer `k_out`,
+ * which must stay valid until the request is done. */
+int eqd_server_submit(eqd_server *server, eqd_grid *grid, const int32_t *cols, int32_t ncols, double *k_out,
+                      int64_t *request_id);
+/* Block until the request is done (EQD_OK), failed (its error), or
+ * `timeout_s` passed (EQD_ERR_TIMEOUT; the request keeps running). */
+int eqd_server_wait(eqd_server *server, int64_t request_id, double timeout_s);
+int eqd_server_poll(eqd_server *server, int64_t request_id, int32_t *done);
+int eqd_server_request_info(eqd_server *server, int64_t request_id, eqd_request_info *info);
+/* Forget a finished request (its id becomes invalid). */
+int eqd_server_release(eqd_server *server, int64_t request_id);
+/* Stops the worker at the end of its current iteration; requests not yet done
+ * are abandoned. Attached grids return to their owner. */
+int eqd_server_destroy(eqd_server *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,7 @@ def test_struct_layouts(built):
     assert C.sizeof(eqd._abi.GridDesc) == 88
     assert C.sizeof(eqd._abi.SolveOpts) == 64
     assert C.sizeof(eqd._abi.Stats) == 72
+    assert C.sizeof(eqd._abi.RequestInfo) == 48
 
 
 def test_defaults_match_reference_cgsolver(built):

@@ -15,6 +15,7 @@ CASES = [
     (12, 10, 9, 1.0, (-1, 1), (-1, 1), 2.0, 1.0, 1.0),             # even n1/n2, shortest axes
     (21, 33, 13, 2.0, (-1, 1), (-1, 1), 2.0, 1.0, 0.5),            # several x2 tiles
     (9, 17, 17, 800.0, (-800, 800), (-800, 800), 32.04e9, 32.04e9, 400.0),  # BP8 scale, h = 100 m
+    (33, 17, 13, 800.0, (-400, 400), (-300, 300), 32.04e9, 32.04e9, 200.0),  # n1 = 33 (h = 25 m lines)
 ]
 
 
