@@ -37,7 +37,24 @@ CONFIGS = {
     "h100": (100.0, 800.0, 800.0, 800.0),   # 17x17x9 (the reference's 17x17x5 case needs >= 9 normal nodes)
     "h50": (50.0, 800.0, 400.0, 800.0),     # 33x33x9, 2,178 columns
     "h20": (20.0, 800.0, 400.0, 800.0),     # 81x81x21, 13,122 columns
+    "h25": (25.0, 1600.0, 800.0, 1600.0),   # 129x129x33, 3.3 M DOF: 2,048 seeded columns + the 10 Toeplitz solves
 }
+# Per-config sample sizes: (K-error check columns, plain single-RHS columns,
+# batched-FP64 columns, CPU-port columns); None = all columns.
+SAMPLES = {
+    "h100": (None, 24, None, 256),
+    "h50": (None, 24, None, 256),
+    "h20": (256, 4, 1024, 16),
+    "h25": (64, 2, 256, 16),
+}
+
+
+def workload_columns(cfg, nf):
+    """The K columns one step builds: all 2nf, or at h = 25 m the 2,048
+    columns drawn without replacement by default_rng(4)."""
+    if cfg == "h25":
+        return np.sort(np.random.default_rng(4).choice(2 * nf, size=2048, replace=False)).astype(np.int32)
+    return np.arange(2 * nf, dtype=np.int32)
 MU = 32.04e9
 NU = 0.25
 
@@ -58,8 +75,10 @@ def workload_name(cfg):
     n1 = int(round(Ln / dz)) + 1
     n23 = int(round(2 * Lf / dz)) + 1
     nf = (int(round(2 * lf / dz)) + 1) ** 2
+    ncols = 2048 if cfg == "h25" else 2 * nf
+    what = f"{ncols} seeded unit-slip columns of {2 * nf}" if ncols != 2 * nf else f"{2 * nf} unit-slip columns"
     return (f"bp8 fault stiffness h={dz:g}m L_fault={Lf:g} L_normal={Ln:g} l_f={lf:g}: "
-            f"{n23}x{n23}x{n1} nodes/side ({6 * n1 * n23 * n23} DOF), {2 * nf} unit-slip columns"), n1, n23, nf
+            f"{n23}x{n23}x{n1} nodes/side ({6 * n1 * n23 * n23} DOF), {what}"), n1, n23, nf
 
 
 def peaks():
@@ -174,7 +193,7 @@ def run_reference(args):
     if rank != 0:
         return
     wl, n1, n23, nf = workload_name(args.config)
-    ofe, ref, cols, nt = cpu_port_sample(args.config, 64 if args.config != "h20" else 8)
+    ofe, ref, cols, nt = cpu_port_sample(args.config, 64 if args.config in ("h100", "h50") else 16)
     for _ in range(args.warmup):
         ref.columns(cols[: max(1, len(cols) // 8)], nthreads=nt)
     t0 = time.perf_counter()
@@ -203,17 +222,26 @@ def main():
     from __graft_entry__ import import_package
     eqd = import_package()
     import torch
+    from eqd_b200.sharding import shard_range
 
     dz, Lf, Ln, lf = CONFIGS[args.config]
     wl, n1, n23, nf = workload_name(args.config)
-    ncols = 2 * nf
-    lo, hi = ncols * rank // world, ncols * (rank + 1) // world
-    cols = np.arange(lo, hi, dtype=np.int32)
+    n_err, n_plain, n_b64, n_cpu = SAMPLES[args.config]
+    all_cols = workload_columns(args.config, nf)
+    ncols = len(all_cols)
+    lo, hi = shard_range(ncols, rank, world)
+    cols = all_cols[lo:hi]
     g = eqd.bp8_grids(dz, Lf, Ln)
-    fe = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="mixed")
+    lam = eqd.lame_lambda(MU, NU)
+    fe = eqd.FaultElasticity(g, lam, MU, lf, device=local, precision="mixed")
     lib = eqd._abi.lib()
     opts = fe.rs.opts()
     opts.itmax = 20000  # safety cap (a converging column needs a few hundred)
+    if args.config in ("h20", "h25"):
+        # Slot pool within 100 GiB (h = 20 m: ~5,000 slots, h = 25 m: ~1,300):
+        # columns refill slots as others finish, and the rest of HBM stays free
+        # for the comparisons below.
+        opts.hbm_budget_bytes = 100 << 30
     kdev = torch.empty((len(cols), 2 * nf), dtype=torch.float64, device=f"cuda:{local}")
 
     def device_step():
@@ -253,10 +281,9 @@ def main():
     mean_it = iters / (args.steps * len(cols))
 
     # End to end through the public API: host K every step.
-    for _ in range(1):
-        Kh = eqd.stiffness_columns(fe, cols)[0]
+    e2e_steps = max(1, min(args.steps, 3 if ncols * nf < 4e7 else 1))
+    Kh = eqd.stiffness_columns(fe, cols)[0]
     t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 3))
     for _ in range(e2e_steps):
         Kh, it_h, st_h = eqd.stiffness_columns(fe, cols)
     e2e_dt = barrier_max(world, (time.perf_counter() - t0) / e2e_steps)
@@ -264,36 +291,12 @@ def main():
            "d2h_bytes_per_step": int(len(cols) * 2 * nf * 8 + len(cols) * 5)}
 
     if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
 
-    # Accuracy of this K against a tight FP64 solve of the same columns (GPU
-    # plain FP64 CG, rtol 1e-12) and against the CPU oracle on a column sample.
     Kmix = kdev.cpu().numpy().T
-    fe64 = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64", rtol=1e-12)
-    K64 = eqd.stiffness_columns(fe64, cols)[0]
-    k_err = float(np.linalg.norm(Kmix - K64) / np.linalg.norm(K64))
-    k_max = float(abs(Kmix - K64).max() / abs(K64).max())
-
-    # Plain FP64 CG, one right-hand side at a time (the comparator).
-    plain = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64", chunk=1)
-    rng = np.random.default_rng(1)
-    sample = np.sort(rng.choice(ncols, size=min(24, ncols), replace=False)).astype(np.int32)
-    eqd.stiffness_columns(plain, sample[:2])
-    t0 = time.perf_counter()
-    lat = []
-    for c in sample:
-        t1 = time.perf_counter()
-        eqd.stiffness_columns(plain, [c])
-        lat.append((time.perf_counter() - t1) * 1e3)
-    plain_v = len(sample) / (time.perf_counter() - t0)
-    # Batched FP64 (same path, all columns) for context.
-    b64 = eqd.FaultElasticity(g, eqd.lame_lambda(MU, NU), MU, lf, device=local, precision="fp64")
-    eqd.stiffness_columns(b64, cols[:64])
-    st64 = eqd._abi.Stats()
-    eqd._abi.check(lib.eqd_stiffness_columns_device(
-        b64.handle, eqd._abi.ptr(cols), C.c_int32(len(cols)), C.byref(b64.rs.opts()),
-        C.c_void_p(kdev.data_ptr()), None, None, C.byref(st64)))
-    batched64_v = len(cols) / st64.device_seconds
 
     # Autotuner evidence: every FP32 launch variant timed on the batch.
     sel = C.c_int32()
@@ -310,7 +313,8 @@ def main():
     # Roofline of the dominant kernel: FP32 stencil apply over the batch.
     ms = C.c_double()
     by = C.c_double()
-    eqd._abi.check(lib.eqd_profile_apply(fe.handle, C.c_int32(len(cols)), C.c_int32(eqd._abi.EQD_PREC_MIXED),
+    napply = min(len(cols), 2178 if args.config in ("h100", "h50") else 512)
+    eqd._abi.check(lib.eqd_profile_apply(fe.handle, C.c_int32(napply), C.c_int32(eqd._abi.EQD_PREC_MIXED),
                                          C.c_int32(3), C.c_int32(10), C.byref(ms), C.byref(by)))
     achieved = by.value / (ms.value * 1e-3) / 1e9
     peak, peak_kind = peaks()
@@ -319,13 +323,100 @@ def main():
     if os.path.exists(tp):
         t = json.load(open(tp)).get(args.config)
         if t:
-            traffic = t["dram_bytes_per_launch_per_column"] * len(cols)
+            traffic = t["dram_bytes_per_launch_per_column"] * napply
+
+    # Time-loop GEMV on the resident K (full square K only).
+    gemv = None
+    if ncols == 2 * nf and 2 * nf <= 524288:  # static-scratch GEMV limit: n * nvec <= 524,288
+        n = 2 * nf
+        nvec = 1
+        s = torch.from_numpy(np.random.default_rng(0).standard_normal(n)).to(kdev.device)
+        y = torch.empty_like(s)
+        stream = torch.cuda.current_stream(kdev.device)
+        Kd = kdev  # row c of kdev = column c of K: column-major K
+        for _ in range(3):
+            eqd._abi.check(lib.eqd_kmat_gemv_static(C.c_int32(local), C.c_int32(n), C.c_void_p(Kd.data_ptr()),
+                                                    C.c_void_p(s.data_ptr()), C.c_void_p(y.data_ptr()),
+                                                    C.c_int32(nvec), C.c_void_p(stream.cuda_stream)))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reps = 20
+        for _ in range(reps):
+            lib.eqd_kmat_gemv_static(C.c_int32(local), C.c_int32(n), C.c_void_p(Kd.data_ptr()),
+                                     C.c_void_p(s.data_ptr()), C.c_void_p(y.data_ptr()), C.c_int32(nvec),
+                                     C.c_void_p(stream.cuda_stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gms = e0.elapsed_time(e1) / reps
+        yref = Kmix @ s.cpu().numpy()
+        gemv = {"n": n, "ms": gms, "GB_s": 8.0 * n * n / (gms * 1e-3) / 1e9,
+                "rel_err_vs_host": float(np.linalg.norm(y.cpu().numpy() - yref) / np.linalg.norm(yref)),
+                "slip": "N(0, 1 m^2), default_rng(0)"}
+
+    # The Toeplitz mode's 10 source solves (src/FaultResponse.jl:339-393:
+    # the centre node, then the four corners, each with s2 and s3) on the
+    # large grid, batched, checked against FP64 single-RHS CG.
+    toeplitz = None
+    if args.config == "h25":
+        n2f = n3f = int(round(np.sqrt(nf)))
+        nodes = [((n3f + 1) // 2 - 1) * n2f + (n2f + 1) // 2 - 1, 0, n2f - 1, (n3f - 1) * n2f, nf - 1]
+        tcols = np.array([k + j * nf for k in nodes for j in (0, 1)], dtype=np.int32)
+        Kt, itt, _ = eqd.stiffness_columns(fe, tcols)
+        t0 = time.perf_counter()
+        Kt, itt, _ = eqd.stiffness_columns(fe, tcols)
+        tdt = time.perf_counter() - t0
+        p1 = eqd.FaultElasticity(g, lam, MU, lf, device=local, precision="fp64", chunk=1, rtol=1e-12)
+        Kt64 = np.column_stack([eqd.stiffness_columns(p1, [c])[0][:, 0] for c in tcols])
+        p1.close()
+        toeplitz = {"solves": int(len(tcols)), "wall_s": tdt, "mean_iterations": float(np.mean(itt)),
+                    "k_rel_err_vs_fp64_single_rhs": float(np.linalg.norm(Kt - Kt64) / np.linalg.norm(Kt64))}
+
+    fe.close()  # release the batch's slot pool before the FP64 comparisons
+
+    # Accuracy of this K against a tight FP64 solve of the same columns (GPU
+    # plain FP64 CG, rtol 1e-12), on all columns or a seeded sample.
+    rng = np.random.default_rng(1)
+    if n_err is None or n_err >= len(cols):
+        pick = np.arange(len(cols))
+    else:
+        pick = np.sort(rng.choice(len(cols), size=n_err, replace=False))
+    fe64 = eqd.FaultElasticity(g, lam, MU, lf, device=local, precision="fp64", rtol=1e-12)
+    K64 = eqd.stiffness_columns(fe64, cols[pick])[0]
+    fe64.close()
+    k_err = float(np.linalg.norm(Kmix[:, pick] - K64) / np.linalg.norm(K64))
+    k_max = float(abs(Kmix[:, pick] - K64).max() / abs(K64).max())
+
+    # Plain FP64 CG, one right-hand side at a time (the comparator).
+    plain = eqd.FaultElasticity(g, lam, MU, lf, device=local, precision="fp64", chunk=1)
+    nz = cols[np.abs(Kmix).sum(0) > 0]  # skip columns whose right-hand side is zero (ring nodes)
+    sample = np.sort(rng.choice(nz, size=min(n_plain, len(nz)), replace=False)).astype(np.int32)
+    eqd.stiffness_columns(plain, sample[:1])
+    t0 = time.perf_counter()
+    lat = []
+    for c in sample:
+        t1 = time.perf_counter()
+        eqd.stiffness_columns(plain, [c])
+        lat.append((time.perf_counter() - t1) * 1e3)
+    plain_v = len(sample) / (time.perf_counter() - t0)
+    plain.close()
+    # Batched FP64 (same path) for context.
+    b64 = eqd.FaultElasticity(g, lam, MU, lf, device=local, precision="fp64")
+    bcols = cols if n_b64 is None or n_b64 >= len(cols) else cols[:n_b64]
+    eqd.stiffness_columns(b64, bcols[:64])
+    st64 = eqd._abi.Stats()
+    eqd._abi.check(lib.eqd_stiffness_columns_device(
+        b64.handle, eqd._abi.ptr(bcols), C.c_int32(len(bcols)), C.byref(b64.rs.opts()),
+        C.c_void_p(kdev.data_ptr()), None, None, C.byref(st64)))
+    batched64_v = len(bcols) / st64.device_seconds
+    b64.close()
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        ofe, ref, ccols, nt = cpu_port_sample(args.config, 256 if args.config != "h20" else 8)
+        ofe, ref, ccols, nt = cpu_port_sample(args.config, n_cpu)
+        ccols = np.intersect1d(ccols, cols) if args.config == "h25" else ccols
         Kc, itc, okc = ref.columns(ccols[:8], nthreads=nt, rtol=1e-13)
-        o_err = float(np.linalg.norm(Kmix[:, ccols[:8]] - Kc) / np.linalg.norm(Kc))
+        pos = np.searchsorted(cols, ccols[:8])
+        o_err = float(np.linalg.norm(Kmix[:, pos] - Kc) / np.linalg.norm(Kc)) if len(pos) and cols[pos[0]] == ccols[0] else None
         t0 = time.perf_counter()
         ref.columns(ccols, nthreads=nt)
         cdt = time.perf_counter() - t0
@@ -341,27 +432,32 @@ def main():
                                                           "determined by the grid)",
         "config": {"workload": wl, "columns": ncols, "precision": "mixed (FP32 CG, FP64 reliable updates)",
                    "rtol": opts.rtol, "parallelism": f"column shards x{world}",
-                   "l2": "inputs larger than L2 (working set %.1f GB)" % (len(cols) * 59400 * 24 / 1e9
-                                                                         if args.config == "h50" else 0),
+                   "l2": "inputs larger than L2 (working set %.1f GB)" % (len(cols) * 6 * n1 * n23 * n23 * 24 / 1e9),
                    "mean_iterations": mean_it},
-        "k_rel_err": {"frobenius_vs_fp64_rtol1e-12": k_err, "max_entry_vs_fp64_rtol1e-12": k_max},
+        "k_rel_err": {"frobenius_vs_fp64_rtol1e-12": k_err, "max_entry_vs_fp64_rtol1e-12": k_max,
+                      "columns_checked": int(len(pick))},
         "solve_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                      "what": "whole-batch build time per step"},
         "plain_fp64_single_rhs": {"value": plain_v, "unit": "columns/s",
                                   "latency_ms_p50": float(np.percentile(lat, 50)),
                                   "latency_ms_p99": float(np.percentile(lat, 99)),
                                   "sample": f"{len(sample)} columns solved one at a time"},
-        "batched_fp64": {"value": batched64_v, "unit": "columns/s"},
+        "batched_fp64": {"value": batched64_v, "unit": "columns/s", "columns": int(len(bcols))},
         "speedup_vs_plain_fp64_single_rhs": value / plain_v,
+        "speedup_vs_batched_fp64": value / batched64_v,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": "plane_march_kernel<float,MODE_A>",
-                     "peak_kind": peak_kind},
+                     "peak_kind": peak_kind, "columns_per_launch": napply},
         "autotune": autotune,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "wall_s_timed": wall,
     }
+    if gemv:
+        line["gemv"] = gemv
+    if toeplitz:
+        line["toeplitz"] = toeplitz
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

@@ -42,6 +42,7 @@ __all__ = [
     "elastic_solver_report", "frictional_node_count", "fault_grid_axes", "shear_traction",
     "fault_stiffness", "fault_stiffness_toeplitz", "stiffness_columns", "apply_operator",
     "KMatrix", "build_model", "EqdError", "EqdArgumentError", "library_path", "Server",
+    "operator_diagonal", "jacobi_preconditioner",
 ]
 
 
@@ -122,7 +123,7 @@ class CGSolver:
     FP64 true residual."""
 
     def __init__(self, fe=None, rtol=1e-10, atol=0.0, itmax=0, precond="none", precision="mixed",
-                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0):
+                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0, split=True):
         if precond not in _PRECONDS:
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precond must be :none or :jacobi, got {precond}")
         if precision not in _PRECISIONS:
@@ -132,6 +133,7 @@ class CGSolver:
         self.precond, self.precision = precond, precision
         self.chunk, self.reliable_delta = int(chunk), float(reliable_delta)
         self.hbm_budget_bytes, self.tile_rows = int(hbm_budget_bytes), int(tile_rows)
+        self.split = bool(split)
         self.stats = CGStats()
         self._warned = False
 
@@ -144,6 +146,8 @@ class CGSolver:
         o.reliable_delta = self.reliable_delta
         o.hbm_budget_bytes = self.hbm_budget_bytes
         o.tile_rows = self.tile_rows
+        if not self.split:
+            o.flags |= _abi.EQD_FLAG_NO_SPLIT
         return o
 
     def record(self, st):
@@ -159,7 +163,7 @@ class CGSolver:
     def duplicate(self):
         """`duplicate(solver)`: same operator and options, fresh counters."""
         return CGSolver(self.fe, self.rtol, self.atol, self.itmax, self.precond, self.precision,
-                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.tile_rows)
+                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.tile_rows, self.split)
 
     def report(self):
         t = self.stats
@@ -284,6 +288,28 @@ def split_node_solve(solver, rhs):
                              None, None, C.byref(st)))
     solver.record(st)
     return U[0].copy() if one else U.T.copy()
+
+
+def operator_diagonal(fe):
+    """diag(A) of the split-node operator A = -H P (D+SAT) P, reference DOF
+    layout, computed on the GPU from the stencil tables (no assembly)."""
+    d = np.empty(fe.Ntot)
+    check(lib().eqd_diag(fe.handle, ptr(d)))
+    return d
+
+
+def jacobi_preconditioner(fe):
+    """`jacobi_preconditioner(A)` (src/ElasticitySplitNode.jl:352-357):
+    1 ./ diag(A), zero entries (the far-field rows) floored to 1; a negative
+    diagonal entry raises."""
+    d = operator_diagonal(fe)
+    if np.any(d < 0):
+        raise EqdArgumentError(_abi.EQD_ERR_ARG, "diag(A) has negative entries; A is not PSD and "
+                                                 "a Jacobi preconditioner would not be SPD")
+    out = np.ones_like(d)
+    nz = d != 0
+    out[nz] = 1.0 / d[nz]
+    return out
 
 
 def apply_operator(fe, x, mode="A", precision="fp64"):

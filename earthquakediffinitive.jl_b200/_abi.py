@@ -25,6 +25,7 @@ EQD_PREC_MIXED = 1
 EQD_PRECOND_NONE = 0
 EQD_PRECOND_JACOBI = 1
 EQD_FLAG_STRICT = 1
+EQD_FLAG_NO_SPLIT = 2
 
 COL_CONVERGED = 1
 COL_MAXITER = 2

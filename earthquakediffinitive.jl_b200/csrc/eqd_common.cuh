@@ -38,6 +38,8 @@ struct ColumnSet {
     const double *slip_dense;  // optional [ncols][2][nf] dense slip (may be null)
     const int8_t *status;      // per-column solve status (null: all active)
     const int8_t *flag;        // per-column "do this step" flag (null: all)
+    const double *dinv;        // MODE_RHS: Jacobi weights (one column, device layout) for
+                               // the second partial sum(dinv y^2); null: none
 };
 
 enum ColStatus : int8_t {

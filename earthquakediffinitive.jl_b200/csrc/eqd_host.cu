@@ -168,7 +168,8 @@ struct Workspace {
     DevBuf newmask, slot_list, dst_list;  // slot engine: entering columns, extraction lists
     DevBuf hbuf;                          // explicit-RHS staging (reference layout)
     cudaGraphExec_t graph = nullptr;
-    int graph_cap = -1, graph_prec = -1, graph_iters = 0, graph_generic = -1, graph_sel = -1;
+    int graph_iters = 0;
+    std::vector<double> graph_key;  // what the captured graph baked in (see SlotRun::setup)
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
     }
@@ -183,6 +184,8 @@ struct eqd_grid {
     MarchCfg m32, m64;
     int m64_maxt = 384;   // launch bound of the FP64 instance the grid runs
     bool served = false;  // attached to an eqd_server (its worker owns the grid)
+    DevBuf dinv64, dinv32;   // Jacobi weights (one column, device layout)
+    bool jacobi_ready = false;
     // FP32 A-apply launch variants (see make_variants) and the chosen one.
     MarchCfg v32[kNumVariants];
     int v32_maxt[kNumVariants] = {};
@@ -192,7 +195,9 @@ struct eqd_grid {
     double tune_ms[kNumVariants] = {};
     int nchunks = 1;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;          // second half of a split batch (graph capture only)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evA = nullptr, evB = nullptr, evFork = nullptr, evJoin = nullptr;
     DevBuf err;           // device error word
     Workspace ws;
     std::mutex mtx;
@@ -233,8 +238,9 @@ static void launch_n1(int n1, dim3 grid, const MarchCfg &m, cudaStream_t st, con
 
 template <typename T, typename TO, int MODE>
 static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols,
-                                int variant = -1) {
+                                int variant = -1, cudaStream_t stream = nullptr) {
     cs.ncols = ncols;
+    cudaStream_t st = stream ? stream : G->stream;
     const int n1 = G->gc.n1;
     if (sizeof(T) == 4 && MODE == MODE_A) {
         const int v = variant >= 0 ? variant : G->sel32;
@@ -244,13 +250,13 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
         const float *fin = reinterpret_cast<const float *>(in);
         float *fout = reinterpret_cast<float *>(out);
         if (lanes == 2)
-            launch_n1<float, float, MODE_A, kMaxT32c, 2>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+            launch_n1<float, float, MODE_A, kMaxT32c, 2>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
                                                           G->err.as<unsigned>());
         else if (G->v32_maxt[v] == kMaxT32)
-            launch_n1<float, float, MODE_A, kMaxT32>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+            launch_n1<float, float, MODE_A, kMaxT32>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
                                                      G->err.as<unsigned>());
         else
-            launch_n1<float, float, MODE_A, kMaxT32b>(n1, grid, m, G->stream, G->c32, fin, fout, cs, partials,
+            launch_n1<float, float, MODE_A, kMaxT32b>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
                                                       G->err.as<unsigned>());
         return cudaGetLastError();
     }
@@ -262,15 +268,15 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
     const bool wide64 = sizeof(T) == 8 && G->m64_maxt == kMaxT64b;
     if (MODE == MODE_AP) {  // generic-input hook: runtime-n1 instance only
         if (wide64)
-            plane_march_kernel<T, TO, MODE, kMaxT64b, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
+            plane_march_kernel<T, TO, MODE, kMaxT64b, 0, 1><<<grid, m.threads, m.smem, st>>>(
                 C, m.g, in, out, cs, partials, G->err.as<unsigned>());
         else
-            plane_march_kernel<T, TO, MODE, MAXT, 0, 1><<<grid, m.threads, m.smem, G->stream>>>(
+            plane_march_kernel<T, TO, MODE, MAXT, 0, 1><<<grid, m.threads, m.smem, st>>>(
                 C, m.g, in, out, cs, partials, G->err.as<unsigned>());
     } else if (wide64) {
-        launch_n1<T, TO, MODE, kMaxT64b>(n1, grid, m, G->stream, C, in, out, cs, partials, G->err.as<unsigned>());
+        launch_n1<T, TO, MODE, kMaxT64b>(n1, grid, m, st, C, in, out, cs, partials, G->err.as<unsigned>());
     } else {
-        launch_n1<T, TO, MODE, MAXT>(n1, grid, m, G->stream, C, in, out, cs, partials, G->err.as<unsigned>());
+        launch_n1<T, TO, MODE, MAXT>(n1, grid, m, st, C, in, out, cs, partials, G->err.as<unsigned>());
     }
     return cudaGetLastError();
 }
@@ -452,8 +458,11 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
         CUDA_OR_RETURN(configure_kernels(optin));
     }
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
+    CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream2, cudaStreamNonBlocking));
     CUDA_OR_RETURN(cudaEventCreate(&G->ev0));
     CUDA_OR_RETURN(cudaEventCreate(&G->ev1));
+    for (cudaEvent_t *e : {&G->evA, &G->evB, &G->evFork, &G->evJoin})
+        CUDA_OR_RETURN(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CUDA_OR_RETURN(G->err.ensure(sizeof(unsigned)));
     CUDA_OR_RETURN(cudaMemset(G->err.p, 0, sizeof(unsigned)));
     *out = G.release();
@@ -470,6 +479,9 @@ extern "C" int eqd_grid_destroy(eqd_grid *G) {
     if (G->stream) cudaStreamSynchronize(G->stream);
     if (G->ev0) cudaEventDestroy(G->ev0);
     if (G->ev1) cudaEventDestroy(G->ev1);
+    for (cudaEvent_t e : {G->evA, G->evB, G->evFork, G->evJoin})
+        if (e) cudaEventDestroy(e);
+    if (G->stream2) cudaStreamDestroy(G->stream2);
     if (G->stream) cudaStreamDestroy(G->stream);
     delete G;
     return EQD_OK;
@@ -626,44 +638,147 @@ static int resolve_chunk(eqd_grid *G, const eqd_solve_opts &o, int ncols, int pr
     return EQD_OK;
 }
 
+// Columns [c0, c0 + n) of the slot arrays, recorded on stream `s`: every
+// pointer is offset to the span, so two spans are independent CG batches.
+struct Span {
+    int c0, n;
+    cudaStream_t s;
+};
+
 template <typename T>
-static void record_iteration(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, const SolveParams &sp,
-                             const ColState &st) {
-    const int nch = G->nchunks;
-    ColumnSet cs{};
-    cs.ncols = cap;
-    cs.slip_node = W.slip_node.as<int>();
-    cs.slip_comp = W.slip_comp.as<int>();
-    cs.slip_dense = W.slip_dense.p ? W.slip_dense.as<double>() : nullptr;
-    cs.status = W.status.as<int8_t>();
-    T *r = W.v0.as<T>(), *p = W.v1.as<T>(), *q = W.v2.as<T>();
+struct IterPtrs {
+    ColumnSet cs;
+    ColState st;
+    T *r, *p, *q;
+    float *d;
+    double *x64, *apply_part, *res_part, *rr_part;
+};
+
+template <typename T>
+static IterPtrs<T> span_ptrs(eqd_grid *G, Workspace &W, const SolveParams &sp, const ColState &st0, const Span &sp_) {
+    const GridConst &gc = G->gc;
+    const long long c0 = sp_.c0;
+    IterPtrs<T> P{};
+    P.cs.ncols = sp_.n;
+    P.cs.slip_node = W.slip_node.as<int>() + c0;
+    P.cs.slip_comp = W.slip_comp.as<int>() + c0;
+    P.cs.slip_dense = W.slip_dense.p ? W.slip_dense.as<double>() + c0 * 2 * gc.nf : nullptr;
+    P.cs.status = W.status.as<int8_t>() + c0;
+    P.st = ColState{st0.gamma + c0, st0.beta + c0, st0.rr_ref + c0, st0.tol + c0, st0.bnorm + c0,
+                    st0.iters + c0, st0.status + c0, st0.flag + c0};
+    P.r = W.v0.as<T>() + c0 * gc.colstride;
+    P.p = W.v1.as<T>() + c0 * gc.colstride;
+    P.q = W.v2.as<T>() + c0 * gc.colstride;
+    P.d = W.v3.p ? W.v3.as<float>() + c0 * gc.colstride : nullptr;
+    P.x64 = W.x64.as<double>() + c0 * gc.colstride;
+    P.apply_part = W.apply_part.as<double>() + c0 * sp.ntiles * 2;
+    P.res_part = W.res_part.as<double>() + c0 * G->m64.g.ntiles * 2;
+    P.rr_part = W.rr_part.as<double>() + c0 * G->nchunks * 2;
+    return P;
+}
+
+// The stencil apply of one CG iteration (q = A p, partial p.q).
+template <typename T>
+static void record_apply(eqd_grid *G, Workspace &W, int generic, const SolveParams &sp, const ColState &st0,
+                         const Span &sn) {
+    IterPtrs<T> P = span_ptrs<T>(G, W, sp, st0, sn);
     if (generic)
-        launch_march<T, T, MODE_AP>(G, p, q, cs, W.apply_part.as<double>(), cap);
+        launch_march<T, T, MODE_AP>(G, P.p, P.q, P.cs, P.apply_part, sn.n, -1, sn.s);
     else
-        launch_march<T, T, MODE_A>(G, p, q, cs, W.apply_part.as<double>(), cap);
-    const unsigned nb = (unsigned)(cap * nch);
+        launch_march<T, T, MODE_A>(G, P.p, P.q, P.cs, P.apply_part, sn.n, -1, sn.s);
+}
+
+// The rest of the iteration: x, r updates; scalars; reliable update (mixed);
+// the next direction.
+template <typename T>
+static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams &sp, const ColState &st0,
+                        const Span &sn) {
+    IterPtrs<T> P = span_ptrs<T>(G, W, sp, st0, sn);
+    const int nch = G->nchunks;
+    const double *dinv64 = sp.precond ? G->dinv64.as<double>() : nullptr;
+    const float *dinv32 = sp.precond ? G->dinv32.as<float>() : nullptr;
+    const unsigned nb = (unsigned)(sn.n * nch);
     if (mixed) {
-        cg_update_kernel<float, float><<<nb, 256, 0, G->stream>>>(W.v3.as<float>(), (float *)r, (const float *)p,
-                                                                 (const float *)q, W.apply_part.as<double>(), st, sp,
-                                                                 W.rr_part.as<double>());
+        cg_update_kernel<float, float><<<nb, 256, 0, sn.s>>>(P.d, (float *)P.r, (const float *)P.p,
+                                                            (const float *)P.q, P.apply_part, P.st, sp, P.rr_part,
+                                                            dinv32);
     } else {
-        cg_update_kernel<double, double><<<nb, 256, 0, G->stream>>>(W.x64.as<double>(), (double *)r,
-                                                                   (const double *)p, (const double *)q,
-                                                                   W.apply_part.as<double>(), st, sp,
-                                                                   W.rr_part.as<double>());
+        cg_update_kernel<double, double><<<nb, 256, 0, sn.s>>>(P.x64, (double *)P.r, (const double *)P.p,
+                                                              (const double *)P.q, P.apply_part, P.st, sp,
+                                                              P.rr_part, dinv64);
     }
-    const unsigned sb = (unsigned)((cap + 127) / 128);
-    cg_scalar_kernel<<<sb, 128, 0, G->stream>>>(st, sp, W.apply_part.as<double>(), W.rr_part.as<double>(), cap, mixed);
+    const unsigned sb = (unsigned)((sn.n + 127) / 128);
+    cg_scalar_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp, P.apply_part, P.rr_part, sn.n, mixed);
     if (mixed) {
-        fold_correction_kernel<<<nb, 256, 0, G->stream>>>(W.x64.as<double>(), W.v3.as<float>(), st, sp);
-        ColumnSet cf = cs;
-        cf.flag = W.flag.as<int8_t>();
-        launch_march<double, float, MODE_RHS>(G, W.x64.as<double>(), (float *)r, cf, W.res_part.as<double>(), cap);
+        fold_correction_kernel<<<nb, 256, 0, sn.s>>>(P.x64, P.d, P.st, sp);
+        ColumnSet cf = P.cs;
+        cf.flag = P.st.flag;
+        cf.dinv = dinv64;
+        launch_march<double, float, MODE_RHS>(G, P.x64, (float *)P.r, cf, P.res_part, sn.n, -1, sn.s);
         SolveParams sp2 = sp;
         sp2.ntiles = G->m64.g.ntiles;
-        cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, W.res_part.as<double>(), cap, 1);
+        cg_true_residual_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp2, P.res_part, sn.n, 1);
     }
-    cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(p, r, st, sp);
+    const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
+    cg_pupdate_kernel<T><<<nb, 256, 0, sn.s>>>(P.p, P.r, P.st, sp, nullptr, dinvT);
+}
+
+// Capture kIter CG iterations over `cap` slots. Large batches are split in
+// two halves on two streams whose stencil applies alternate: the
+// arithmetic-bound apply of one half runs while the memory-bound vector
+// updates of the other half stream through HBM.
+template <typename T>
+static void record_iterations(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, const SolveParams &sp,
+                              const ColState &st, int kIter, bool split) {
+    if (!split) {
+        const Span all{0, cap, G->stream};
+        for (int k = 0; k < kIter; ++k) {
+            record_apply<T>(G, W, generic, sp, st, all);
+            record_rest<T>(G, W, mixed, sp, st, all);
+        }
+        return;
+    }
+    const int h0 = cap / 2;
+    const Span A{0, h0, G->stream}, B{h0, cap - h0, G->stream2};
+    cudaEventRecord(G->evFork, A.s);
+    cudaStreamWaitEvent(B.s, G->evFork, 0);
+    for (int k = 0; k < kIter; ++k) {
+        if (k > 0) cudaStreamWaitEvent(A.s, G->evB, 0);  // B's previous apply is done
+        record_apply<T>(G, W, generic, sp, st, A);
+        cudaEventRecord(G->evA, A.s);
+        cudaStreamWaitEvent(B.s, G->evA, 0);             // B's apply follows A's
+        record_apply<T>(G, W, generic, sp, st, B);
+        cudaEventRecord(G->evB, B.s);
+        record_rest<T>(G, W, mixed, sp, st, A);
+        record_rest<T>(G, W, mixed, sp, st, B);
+    }
+    cudaEventRecord(G->evJoin, B.s);
+    cudaStreamWaitEvent(A.s, G->evJoin, 0);
+}
+
+// Jacobi weights dinv = 1 / diag(A) (zeros floored to 1), computed once per
+// grid; a negative diagonal entry is an error, as in the reference.
+static int ensure_jacobi(eqd_grid *G) {
+    if (G->jacobi_ready) return EQD_OK;
+    const GridConst &gc = G->gc;
+    CUDA_OR_RETURN(G->dinv64.ensure(sizeof(double) * gc.colstride));
+    CUDA_OR_RETURN(G->dinv32.ensure(sizeof(float) * gc.colstride));
+    CUDA_OR_RETURN(cudaMemsetAsync(G->dinv64.p, 0, sizeof(double) * gc.colstride, G->stream));
+    CUDA_OR_RETURN(cudaMemsetAsync(G->dinv32.p, 0, sizeof(float) * gc.colstride, G->stream));
+    DevBuf neg;
+    CUDA_OR_RETURN(neg.ensure(sizeof(unsigned)));
+    CUDA_OR_RETURN(cudaMemsetAsync(neg.p, 0, sizeof(unsigned), G->stream));
+    const long long n = 6LL * gc.n1 * gc.n2 * gc.n3;
+    jacobi_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, G->stream>>>(
+        G->c64, gc.n1, gc.n2, gc.n3, gc.PS, nullptr, G->dinv64.as<double>(), G->dinv32.as<float>(), neg.as<unsigned>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    unsigned h = 0;
+    CUDA_OR_RETURN(cudaMemcpyAsync(&h, neg.p, sizeof(unsigned), cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    if (h) return fail(EQD_ERR_ARG, "diag(A) has negative entries; A is not PSD and a Jacobi preconditioner "
+                                    "would not be SPD");
+    G->jacobi_ready = true;
+    return EQD_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -760,7 +875,7 @@ struct SlotRun {
         for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
         CUDA_OR_RETURN(w.apply_part.ensure(sizeof(double) * 2 * cap * ntmax));
         CUDA_OR_RETURN(w.res_part.ensure(sizeof(double) * 2 * cap * std::max(nt64, G->nchunks)));
-        CUDA_OR_RETURN(w.rr_part.ensure(sizeof(double) * cap * G->nchunks));
+        CUDA_OR_RETURN(w.rr_part.ensure(sizeof(double) * 2 * cap * G->nchunks));
         for (DevBuf *b : {&w.gamma, &w.beta, &w.rr_ref, &w.tol, &w.bnorm}) CUDA_OR_RETURN(b->ensure(sizeof(double) * cap));
         CUDA_OR_RETURN(w.iters.ensure(sizeof(int) * cap));
         CUDA_OR_RETURN(w.status.ensure(cap));
@@ -786,6 +901,11 @@ struct SlotRun {
         sp.nchunks = G->nchunks;
         sp.colstride = gc.colstride;
         sp.ntot = ntot;
+        sp.precond = o.precond == EQD_PRECOND_JACOBI;
+        if (sp.precond) {
+            int rc = ensure_jacobi(G);
+            if (rc) return rc;
+        }
         itmax = o.itmax > 0 ? o.itmax : 2 * ntot;
 
         // Every slot starts free: status IDLE everywhere, vectors zeroed as
@@ -803,23 +923,35 @@ struct SlotRun {
         CUDA_OR_RETURN(cudaMemsetAsync(w.flag.p, 0, cap, G->stream));
 
         // Graph of kIter iterations over all slots, captured once per
-        // (capacity, precision, mode, launch variant).
-        if (!w.graph || w.graph_cap != cap || w.graph_prec != o.precision || w.graph_generic != generic ||
-            w.graph_sel != G->sel32) {
+        // (capacity, precision, mode, launch variant, preconditioner, split).
+        const bool split = cap >= 64 && !(o.flags & EQD_FLAG_NO_SPLIT);
+        // Everything the captured kernels bake in: sizes, options and every
+        // workspace pointer (a buffer that grew or was released since the
+        // capture must not be reached through the old graph).
+        const double key[] = {(double)cap, (double)o.precision, (double)generic, (double)G->sel32,
+                              (double)o.precond, (double)split, sp.rtol, sp.atol, (double)sp.itmax, sp.delta,
+                              (double)(uintptr_t)w.x64.p, (double)(uintptr_t)w.v0.p, (double)(uintptr_t)w.v1.p,
+                              (double)(uintptr_t)w.v2.p, (double)(uintptr_t)w.v3.p, (double)(uintptr_t)w.apply_part.p,
+                              (double)(uintptr_t)w.res_part.p, (double)(uintptr_t)w.rr_part.p,
+                              (double)(uintptr_t)w.gamma.p, (double)(uintptr_t)w.beta.p, (double)(uintptr_t)w.rr_ref.p,
+                              (double)(uintptr_t)w.tol.p, (double)(uintptr_t)w.bnorm.p, (double)(uintptr_t)w.iters.p,
+                              (double)(uintptr_t)w.status.p, (double)(uintptr_t)w.flag.p,
+                              (double)(uintptr_t)w.slip_node.p, (double)(uintptr_t)w.slip_comp.p,
+                              (double)(uintptr_t)w.slip_dense.p, (double)(uintptr_t)G->dinv64.p,
+                              (double)(uintptr_t)G->dinv32.p};
+        const std::vector<double> kv(std::begin(key), std::end(key));
+        if (!w.graph || w.graph_key != kv) {
             if (w.graph) cudaGraphExecDestroy(w.graph);
             w.graph = nullptr;
             cudaGraph_t g;
             CUDA_OR_RETURN(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; k < kIter; ++k) record_iteration<T>(G, w, cap, mixed, generic, sp, st);
+            record_iterations<T>(G, w, cap, mixed, generic, sp, st, kIter, split);
             cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
             ce = cudaGraphInstantiate(&w.graph, g, 0);
             cudaGraphDestroy(g);
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-            w.graph_cap = cap;
-            w.graph_prec = o.precision;
-            w.graph_generic = generic;
-            w.graph_sel = G->sel32;
+            w.graph_key = kv;
             w.graph_iters = kIter;
         }
         return EQD_OK;
@@ -884,6 +1016,7 @@ struct SlotRun {
             // r0 = b = H P (D+SAT) chi  (x = 0), in the working precision.
             ColumnSet cs = colset();
             cs.flag = mask;
+            cs.dinv = sp.precond ? G->dinv64.as<double>() : nullptr;
             CUDA_OR_RETURN((launch_march<double, T, MODE_RHS>(G, w.x64.as<double>(), w.v0.as<T>(), cs,
                                                                w.res_part.as<double>(), cap)));
             SolveParams sp2 = sp;
@@ -904,13 +1037,16 @@ struct SlotRun {
                 ++launches;
             }
             column_sumsq_kernel<T><<<nb, 256, 0, G->stream>>>(w.v0.as<T>(), cst, G->nchunks, mask,
-                                                               w.res_part.as<double>());
+                                                               w.res_part.as<double>(),
+                                                               sp.precond ? G->dinv64.as<double>() : nullptr);
             SolveParams sp2 = sp;
             sp2.ntiles = G->nchunks;
             cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, w.res_part.as<double>(), cap, 0, mask);
             launches += 2;
         }
-        cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), w.v0.as<T>(), st, sp, mask);
+        const T *dinvT = !sp.precond ? nullptr
+                                     : (const T *)(sizeof(T) == 4 ? (const void *)G->dinv32.p : (const void *)G->dinv64.p);
+        cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), w.v0.as<T>(), st, sp, mask, dinvT);
         ++launches;
         CUDA_OR_RETURN(cudaGetLastError());
         return EQD_OK;
@@ -1106,9 +1242,8 @@ static int run_batch_any(eqd_grid *G, const eqd_solve_opts *opts, const BatchSpe
     if (opts) o = *opts;
     else eqd_default_opts(&o);
     if (!(o.rtol >= 0) || !(o.atol >= 0)) return fail(EQD_ERR_ARG, "rtol/atol must be non-negative");
-    if (o.precond == EQD_PRECOND_JACOBI)
-        return fail(EQD_ERR_UNSUPPORTED, "precond=:jacobi is not available on this path");
-    if (o.precond != EQD_PRECOND_NONE) return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
+    if (o.precond != EQD_PRECOND_NONE && o.precond != EQD_PRECOND_JACOBI)
+        return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
     if (o.precision != EQD_PREC_FP64 && o.precision != EQD_PREC_MIXED) return fail(EQD_ERR_ARG, "unknown precision");
     if (B.rhs && o.precision != EQD_PREC_FP64) return fail(EQD_ERR_UNSUPPORTED, "explicit-RHS solves run in FP64");
     const auto t0 = std::chrono::steady_clock::now();
@@ -1333,9 +1468,26 @@ extern "C" int eqd_set_variant(eqd_grid *G, int32_t variant) {
 }
 
 extern "C" int eqd_diag(eqd_grid *G, double *d) {
-    (void)G;
-    (void)d;
-    return fail(EQD_ERR_UNSUPPORTED, "eqd_diag is not implemented yet");
+    if (!G || !d) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    const GridConst &gc = G->gc;
+    const long long n = 6LL * gc.n1 * gc.n2 * gc.n3;
+    DevBuf dev, ref, neg;
+    CUDA_OR_RETURN(dev.ensure(sizeof(double) * gc.colstride));
+    CUDA_OR_RETURN(ref.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(neg.ensure(sizeof(unsigned)));
+    CUDA_OR_RETURN(cudaMemsetAsync(neg.p, 0, sizeof(unsigned), G->stream));
+    jacobi_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, G->stream>>>(G->c64, gc.n1, gc.n2, gc.n3, gc.PS,
+                                                                            dev.as<double>(), nullptr, nullptr,
+                                                                            neg.as<unsigned>());
+    dev_to_ref_kernel<double, double><<<(unsigned)((n + 255) / 256), 256, 0, G->stream>>>(
+        dev.as<double>(), ref.as<double>(), gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, 1);
+    CUDA_OR_RETURN(cudaGetLastError());
+    CUDA_OR_RETURN(cudaMemcpyAsync(d, ref.p, sizeof(double) * n, cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    return EQD_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1644,9 +1796,8 @@ extern "C" int eqd_server_create(const eqd_solve_opts *opts, uint64_t hbm_budget
     const eqd_solve_opts &o = S->opts;
     if (!(o.rtol >= 0) || !(o.atol >= 0)) return fail(EQD_ERR_ARG, "rtol/atol must be non-negative");
     if (o.precision != EQD_PREC_FP64 && o.precision != EQD_PREC_MIXED) return fail(EQD_ERR_ARG, "unknown precision");
-    if (o.precond == EQD_PRECOND_JACOBI)
-        return fail(EQD_ERR_UNSUPPORTED, "precond=:jacobi is not available on this path");
-    if (o.precond != EQD_PRECOND_NONE) return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
+    if (o.precond != EQD_PRECOND_NONE && o.precond != EQD_PRECOND_JACOBI)
+        return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
     S->budget = hbm_budget_bytes;
     if (S->budget == 0) {
         size_t fr = 0, tot = 0;

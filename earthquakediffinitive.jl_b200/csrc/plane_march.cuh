@@ -680,9 +680,10 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 const T va = v1w[l][3], vb = v2w[l][3];
                 if (MODE == MODE_RHS) {
                     acc0[l] += (double)y1 * (double)y1 + (double)y2 * (double)y2;
-                } else if (sizeof(T) == 4) {
-                    acc0[l] += (double)(va * y1 + vb * y2);
-                    acc1[l] += (double)(va * va + vb * vb);
+                    if (cs.dinv) {
+                        const double *dv = cs.dinv + poff + (long long)p * g.PS;
+                        acc1[l] += dv[0] * (double)y1 * (double)y1 + dv[cstr] * (double)y2 * (double)y2;
+                    }
                 } else {
                     acc0[l] += (double)va * (double)y1 + (double)vb * (double)y2;
                     acc1[l] += (double)va * (double)va + (double)vb * (double)vb;
@@ -704,9 +705,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 const T vc = v3w[l][0];
                 if (MODE == MODE_RHS) {
                     acc0[l] += (double)y3 * (double)y3;
-                } else if (sizeof(T) == 4) {
-                    acc0[l] += (double)(vc * y3);
-                    acc1[l] += (double)(vc * vc);
+                    if (cs.dinv) acc1[l] += cs.dinv[poff + 2 * cstr + (long long)z * g.PS] * (double)y3 * (double)y3;
                 } else {
                     acc0[l] += (double)vc * (double)y3;
                     acc1[l] += (double)vc * (double)vc;

@@ -29,6 +29,7 @@ struct SolveParams {
     int nchunks;        // update partials per column
     long long colstride;
     long long ntot;     // unpadded DOF count (for itmax default)
+    int precond;        // 1: Jacobi (gamma = r.z, z = dinv r); 0: none (z = r)
 };
 
 // ---------------------------------------------------------------------------
@@ -36,11 +37,14 @@ struct SolveParams {
 // X is the solution accumulator (FP64 for plain CG, FP32 correction d for the
 // mixed inner solve).
 // ---------------------------------------------------------------------------
+// rr_part[col][chunk][2] = (r.r, r.z) partials; r.z = r.r without a
+// preconditioner (`dinv` null), z = dinv r with one (Jacobi).
 template <typename T, typename TX>
 __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *__restrict__ r,
                                                         const T *__restrict__ p, const T *__restrict__ q,
                                                         const double *__restrict__ apply_part, ColState st,
-                                                        SolveParams sp, double *__restrict__ rr_part) {
+                                                        SolveParams sp, double *__restrict__ rr_part,
+                                                        const T *__restrict__ dinv = nullptr) {
     const int col = blockIdx.x / sp.nchunks;
     const int chunk = blockIdx.x % sp.nchunks;
     if (st.status[col] != COL_ACTIVE) return;
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
     const long long n = sp.colstride;
     const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
     const long long off = (long long)col * n;
-    double acc = 0.0;
+    double acc = 0.0, accz = 0.0;
     const T a_t = (T)alpha;
     for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
         const T pi = p[off + i], qi = q[off + i];
@@ -69,16 +73,27 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
         const T ri = r[off + i] - a_t * qi;
         r[off + i] = ri;
         acc += (double)ri * (double)ri;
+        if (dinv) accz += (double)dinv[i] * (double)ri * (double)ri;
     }
     const double s = block_sum(acc, red);
-    if (threadIdx.x == 0) rr_part[(long long)col * sp.nchunks + chunk] = s;
+    double sz = s;
+    if (dinv) {
+        __syncthreads();
+        sz = block_sum(accz, red);
+    }
+    if (threadIdx.x == 0) {
+        rr_part[((long long)col * sp.nchunks + chunk) * 2 + 0] = s;
+        rr_part[((long long)col * sp.nchunks + chunk) * 2 + 1] = sz;
+    }
 }
 
 // p = r + beta p for active columns (only the masked ones when `mask` is set:
 // the first direction of columns that just entered the batch).
+// With a preconditioner: p = dinv r + beta p.
 template <typename T>
 __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, const T *__restrict__ r, ColState st,
-                                                         SolveParams sp, const int8_t *__restrict__ mask = nullptr) {
+                                                         SolveParams sp, const int8_t *__restrict__ mask = nullptr,
+                                                         const T *__restrict__ dinv = nullptr) {
     const int col = blockIdx.x / sp.nchunks;
     const int chunk = blockIdx.x % sp.nchunks;
     if (st.status[col] != COL_ACTIVE) return;
@@ -87,7 +102,12 @@ __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, cons
     const long long n = sp.colstride;
     const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
     const long long off = (long long)col * n;
-    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) p[off + i] = r[off + i] + b * p[off + i];
+    if (dinv) {
+        for (long long i = beg + threadIdx.x; i < end; i += blockDim.x)
+            p[off + i] = dinv[i] * r[off + i] + b * p[off + i];
+    } else {
+        for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) p[off + i] = r[off + i] + b * p[off + i];
+    }
 }
 
 // Mixed precision: fold the FP32 correction into the FP64 solution.
@@ -119,7 +139,8 @@ __global__ void cg_scalar_kernel(ColState st, SolveParams sp, const double *__re
     if (col >= ncols || st.status[col] != COL_ACTIVE) return;
     const double pq = sum_parts(apply_part, col, sp.ntiles, 2, 0);
     const double pp = sum_parts(apply_part, col, sp.ntiles, 2, 1);
-    const double rr = sum_parts(rr_part, col, sp.nchunks, 1, 0);
+    const double rr = sum_parts(rr_part, col, sp.nchunks, 2, 0);
+    const double rz = sum_parts(rr_part, col, sp.nchunks, 2, 1);
     const long long itmax = sp.itmax > 0 ? sp.itmax : 2 * sp.ntot;
     const int it = st.iters[col] + 1;
     st.iters[col] = it;
@@ -141,8 +162,8 @@ __global__ void cg_scalar_kernel(ColState st, SolveParams sp, const double *__re
         } else if (it >= itmax) {
             st.status[col] = COL_MAXITER;
         } else {
-            st.beta[col] = rr / st.gamma[col];
-            st.gamma[col] = rr;
+            st.beta[col] = rz / st.gamma[col];
+            st.gamma[col] = rz;
         }
         return;
     }
@@ -150,8 +171,8 @@ __global__ void cg_scalar_kernel(ColState st, SolveParams sp, const double *__re
     if (rr <= tol * tol || rr <= sp.delta * sp.delta * st.rr_ref[col] || it >= itmax) {
         st.flag[col] = 1;
     } else {
-        st.beta[col] = rr / st.gamma[col];
-        st.gamma[col] = rr;
+        st.beta[col] = rz / st.gamma[col];
+        st.gamma[col] = rz;
         st.flag[col] = 0;
     }
 }
@@ -166,13 +187,14 @@ __global__ void cg_true_residual_kernel(ColState st, SolveParams sp, const doubl
     if (col >= ncols || st.status[col] != COL_ACTIVE) return;
     if (mask ? !mask[col] : (mixed && !st.flag[col])) return;
     const double rr = sum_parts(res_part, col, sp.ntiles, 2, 0);
+    const double rz = sp.precond ? sum_parts(res_part, col, sp.ntiles, 2, 1) : rr;
     const int it = st.iters[col];
     if (it == 0) {
         const double bn = sqrt(rr);
         st.bnorm[col] = bn;
         st.tol[col] = sp.atol + sp.rtol * bn;
         st.beta[col] = 0.0;
-        st.gamma[col] = rr;
+        st.gamma[col] = rz;
         st.rr_ref[col] = rr;
         st.flag[col] = 0;
         if (rr == 0.0) st.status[col] = COL_CONVERGED;  // x = 0 solves it exactly
@@ -189,8 +211,8 @@ __global__ void cg_true_residual_kernel(ColState st, SolveParams sp, const doubl
     } else if (it >= itmax) {
         st.status[col] = COL_MAXITER;
     } else {
-        st.beta[col] = rr / st.gamma[col];
-        st.gamma[col] = rr;
+        st.beta[col] = rz / st.gamma[col];
+        st.gamma[col] = rz;
         st.rr_ref[col] = rr;
     }
 }
@@ -212,20 +234,107 @@ __global__ void __launch_bounds__(256) zero_columns_kernel(T *__restrict__ v, lo
 // stencil's [column][chunk][2] (slot 0) so cg_true_residual_kernel reads them.
 template <typename T>
 __global__ void __launch_bounds__(256) column_sumsq_kernel(const T *__restrict__ v, long long colstride, int nchunks,
-                                                           const int8_t *__restrict__ mask, double *__restrict__ part) {
+                                                           const int8_t *__restrict__ mask, double *__restrict__ part,
+                                                           const double *__restrict__ dinv = nullptr) {
     const int col = blockIdx.x / nchunks;
     const int chunk = blockIdx.x % nchunks;
     if (!mask[col]) return;
     __shared__ double red[32];
     const long long beg = colstride * chunk / nchunks, end = colstride * (chunk + 1) / nchunks;
     const T *vc = v + (long long)col * colstride;
-    double acc = 0.0;
-    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) acc += (double)vc[i] * (double)vc[i];
+    double acc = 0.0, accz = 0.0;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        acc += (double)vc[i] * (double)vc[i];
+        if (dinv) accz += dinv[i] * (double)vc[i] * (double)vc[i];
+    }
     const double s = block_sum(acc, red);
+    double sz = 0.0;
+    if (dinv) {
+        __syncthreads();
+        sz = block_sum(accz, red);
+    }
     if (threadIdx.x == 0) {
         part[((long long)col * nchunks + chunk) * 2 + 0] = s;
-        part[((long long)col * nchunks + chunk) * 2 + 1] = 0.0;
+        part[((long long)col * nchunks + chunk) * 2 + 1] = sz;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi: diag(A) of A = -H P (D + SAT) P, one thread per DOF, device layout
+// (`jacobi_preconditioner`, src/ElasticitySplitNode.jl:352-357, takes it from
+// the assembled A). For comp j at a node off the fault face,
+//   A_nn = -H_n (mu (D2_1 + D2_2 + D2_3) + mu D2_j + lam W_j)_nn ;
+// at a fault pair (m minus, p plus; P averages both inputs and outputs)
+//   A_mm = A_pp = -H_m/4 (D_mm + D_pp + 2c (t+ - t-)),
+// t = d tau_j / d v_j at the own face node (tau on the fixed +x1 axis);
+// far-field rows are zero. W = D1 D1 entries come from the D1 rows.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double d1_entry(const AxisT<double> &a, int n, int i, int k) {
+    const int o = k - i;
+    if (i < 4) return (o >= -3 && o <= 3) ? a.d1_cl[i][o + 3] : 0.0;
+    if (i >= n - 4) return (o >= -3 && o <= 3) ? a.d1_cl[4 + (n - 1 - i)][o + 3] : 0.0;
+    return (o >= -2 && o <= 2) ? a.d1_int[o + 2] : 0.0;
+}
+
+__device__ __forceinline__ double d2_diag(const AxisT<double> &a, int n, int i) {
+    if (i < 4) return a.d2_cl[i][3];
+    if (i >= n - 4) return a.d2_cl[4 + (n - 1 - i)][3];
+    return a.d2_int[2];
+}
+
+__device__ __forceinline__ double w_diag(const AxisT<double> &a, int n, int i) {
+    double s = 0.0;
+    for (int k = max(i - 3, 0); k <= min(i + 3, n - 1); ++k) s += d1_entry(a, n, i, k) * d1_entry(a, n, k, i);
+    return s;
+}
+
+__device__ __forceinline__ double hq(const AxisT<double> &a, int n, int i) {
+    if (i < 4) return a.wq[i];
+    if (i >= n - 4) return a.wq[n - 1 - i];
+    return 1.0;
+}
+
+__global__ void jacobi_diag_kernel(const __grid_constant__ OpConst<double> C, int n1, int n2, int n3, int PS,
+                                   double *__restrict__ diag, double *__restrict__ dinv64, float *__restrict__ dinv32,
+                                   unsigned *__restrict__ negative) {
+    const long long N = (long long)n1 * n2 * n3;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= 6 * N) return;
+    const int sc = (int)(gid / N);
+    const long long pt = gid % N;
+    const int side = sc / 3, j = sc % 3;
+    const int i3 = (int)(pt / ((long long)n1 * n2));
+    const int i2 = (int)((pt / n1) % n2);
+    const int i1 = (int)(pt % n1);
+    const long long idx = ((long long)sc * n3 + i3) * PS + (long long)i2 * n1 + i1;
+    const bool ff = (side == 0 && i1 == 0) || (side == 1 && i1 == n1 - 1) || i2 == 0 || i2 == n2 - 1 || i3 == 0 ||
+                    i3 == n3 - 1;
+    double d = 0.0;
+    if (!ff) {
+        const int nn[3] = {n1, n2, n3};
+        auto Djj = [&](int a1) {
+            const int ii[3] = {a1, i2, i3};
+            double lap = 0.0;
+            for (int a = 0; a < 3; ++a) lap += d2_diag(C.ax[a], nn[a], ii[a]);
+            return C.mu * (lap + d2_diag(C.ax[j], nn[j], ii[j])) + C.lam * w_diag(C.ax[j], nn[j], ii[j]);
+        };
+        const double H = C.hvol * hq(C.ax[0], n1, i1) * hq(C.ax[1], n2, i2) * hq(C.ax[2], n3, i3);
+        const bool face = (side == 0 && i1 == n1 - 1) || (side == 1 && i1 == 0);
+        if (!face) {
+            d = -H * Djj(i1);
+        } else {
+            const AxisT<double> &A1 = C.ax[0];
+            const double dt = j == 0 ? C.lam * (d1_entry(A1, n1, 0, 0) - d1_entry(A1, n1, n1 - 1, n1 - 1)) +
+                                           4.0 * C.mu * A1.dlo[0]
+                                     : 2.0 * C.mu * A1.dlo[0];
+            d = -0.25 * H * (Djj(n1 - 1) + Djj(0) + 2.0 * C.sat_c * dt);
+        }
+    }
+    if (d < 0.0) atomicOr(negative, 1u);
+    const double inv = d > 0.0 ? 1.0 / d : 1.0;
+    if (diag) diag[idx] = d;
+    if (dinv64) dinv64[idx] = inv;
+    if (dinv32) dinv32[idx] = (float)inv;
 }
 
 __global__ void count_active_kernel(const int8_t *__restrict__ status, int ncols, int *__restrict__ out) {

@@ -11,7 +11,8 @@ the reference package.
 module EqdB200
 
 export GpuFaultElasticity, gpu_fault_stiffness, gpu_fault_stiffness_toeplitz,
-       gpu_shear_traction, GpuK, gpu_mul!, gpu_solver_report
+       gpu_shear_traction, GpuK, gpu_mul!, gpu_solver_report,
+       GpuServer, serve!, submit, wait_request, request_info
 
 const libeqd = get(ENV, "EQD_LIB", joinpath(@__DIR__, "..", "lib", "libeqd.so"))
 
@@ -154,6 +155,60 @@ function gpu_mul!(y::Vector{Float64}, K::GpuK, s::Vector{Float64})
     check(ccall((:eqd_kmat_gemv, libeqd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
                 K.handle, s, y, 1))
     return y
+end
+
+# ---------------------------------------------------------------------------
+# Request serving (eqd_server_*): continuous batching of K-column requests
+# ---------------------------------------------------------------------------
+struct RequestInfo
+    state::Int32; ncols::Int32; unconverged::Int32; max_iterations::Int32
+    iterations::Int64; t_submit::Float64; t_start::Float64; t_done::Float64
+end
+
+mutable struct GpuServer
+    handle::Ptr{Cvoid}
+    outputs::Dict{Int64,Matrix{Float64}}   # keeps each request's K buffer alive
+end
+
+function GpuServer(; hbm_budget_bytes=150_000_000_000, solver_kwargs...)
+    o = default_opts(; solver_kwargs...)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:eqd_server_create, libeqd), Cint, (Ref{SolveOpts}, UInt64, Ref{Ptr{Cvoid}}),
+                o, UInt64(hbm_budget_bytes), h))
+    s = GpuServer(h[], Dict{Int64,Matrix{Float64}}())
+    finalizer(s) do x
+        x.handle == C_NULL || ccall((:eqd_server_destroy, libeqd), Cint, (Ptr{Cvoid},), x.handle)
+        x.handle = C_NULL
+    end
+    return s
+end
+
+"Attach a grid (it belongs to the server from now on); `slots = 0` sizes the slot pool from the budget."
+serve!(s::GpuServer, fe::GpuFaultElasticity; slots=0) =
+    check(ccall((:eqd_server_add_grid, libeqd), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Int32), s.handle, fe.handle, slots))
+
+"Queue K columns `cols` (1-based, as K's column indices) of an attached grid; returns the request id."
+function submit(s::GpuServer, fe::GpuFaultElasticity, cols::AbstractVector{<:Integer})
+    out = Matrix{Float64}(undef, 2fe.nf, length(cols))
+    id = Ref{Int64}(0)
+    c = Int32.(cols .- 1)
+    check(ccall((:eqd_server_submit, libeqd), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Int32}, Int32, Ptr{Float64}, Ref{Int64}),
+                s.handle, fe.handle, c, length(c), out, id))
+    s.outputs[id[]] = out
+    return id[]
+end
+
+"Block until the request is done; returns its K columns (2nf x length(cols))."
+function wait_request(s::GpuServer, id::Int64; timeout=-1.0)
+    check(ccall((:eqd_server_wait, libeqd), Cint, (Ptr{Cvoid}, Int64, Float64), s.handle, id, timeout))
+    return s.outputs[id]
+end
+
+function request_info(s::GpuServer, id::Int64)
+    r = Ref{RequestInfo}()
+    check(ccall((:eqd_server_request_info, libeqd), Cint, (Ptr{Cvoid}, Int64, Ref{RequestInfo}), s.handle, id, r))
+    return r[]
 end
 
 end # module

@@ -64,13 +64,16 @@ class Server:
     `rtol`, ...; the same keywords as `CGSolver`), slot pools within
     `hbm_budget_bytes` (0: free device memory minus 2 GiB)."""
 
-    def __init__(self, hbm_budget_bytes=0, rtol=1e-10, atol=0.0, itmax=0, precision="mixed", reliable_delta=0.01):
+    def __init__(self, hbm_budget_bytes=0, rtol=1e-10, atol=0.0, itmax=0, precision="mixed", reliable_delta=0.01,
+                 split=True):
         o = _abi.default_opts()
         o.rtol, o.atol, o.itmax = float(rtol), float(atol), int(itmax)
         if precision not in ("mixed", "fp64"):
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precision must be 'mixed' or 'fp64', got {precision}")
         o.precision = _abi.EQD_PREC_MIXED if precision == "mixed" else _abi.EQD_PREC_FP64
         o.reliable_delta = float(reliable_delta)
+        if not split:
+            o.flags |= _abi.EQD_FLAG_NO_SPLIT
         h = C.c_void_p()
         check(lib().eqd_server_create(C.byref(o), C.c_uint64(int(hbm_budget_bytes)), C.byref(h)))
         self._h = h

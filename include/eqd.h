@@ -59,6 +59,8 @@ typedef enum {
 typedef enum { EQD_PRECOND_NONE = 0, EQD_PRECOND_JACOBI = 1 } eqd_precond;
 
 #define EQD_FLAG_STRICT 1u    /* return EQD_ERR_NOT_CONVERGED if any column did not converge */
+#define EQD_FLAG_NO_SPLIT 2u  /* run a large batch as one chain of kernels instead of two halves whose
+                                 stencil applies alternate (for comparisons; results are identical) */
 
 /*
  * Two equidistant blocks meeting at the fault plane x1 = 0:

@@ -180,3 +180,38 @@ def test_slot_refill_equals_full_batch(eqd, precision):
     assert (sta == stf).all()
     r = eqd.solver_report(fe_few.rs)
     assert r["solves"] == len(cols) and r["unconverged"] == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_split_halves_equal_single_chain(eqd, precision):
+    """A batch of >= 64 columns runs as two halves on two streams whose
+    stencil applies alternate; the K columns and iteration counts are the
+    same bits as one chain of kernels."""
+    kw = dict(precision=precision)
+    fe_s = eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.6, **kw)
+    fe_1 = eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.6, split=False, **kw)
+    for fe in (fe_s, fe_1):
+        eqd.set_stencil_variant(fe, 1)
+    cols = np.arange(2 * fe_s.nf)
+    assert len(cols) >= 64
+    Ks, its, _ = eqd.stiffness_columns(fe_s, cols)
+    K1, it1, _ = eqd.stiffness_columns(fe_1, cols)
+    assert np.array_equal(Ks, K1) and np.array_equal(its, it1)
+
+
+def test_mixed_corner_columns_bp8_scale(eqd):
+    """BP8 units at h = 100 m with Omega_f = the whole fault plane: the
+    columns next to the corners of the fault have right-hand sides whose
+    dot-product terms exceed the FP32 range (|b_i q_i| ~ 5e38); the mixed
+    solve must still converge to the FP64 K (dot products in FP64)."""
+    mu = 32.04e9
+    g = eqd.bp8_grids(100.0, 800.0, 800.0)
+    fe = eqd.FaultElasticity(g, eqd.lame_lambda(mu, 0.25), mu, 800.0, precision="mixed", itmax=5000)
+    fe64 = eqd.FaultElasticity(g, eqd.lame_lambda(mu, 0.25), mu, 800.0, precision="fp64", rtol=1e-12)
+    nf = fe.nf
+    corners = [18, 32, 256, 270]
+    cols = np.array(corners + [c + nf for c in corners] + [144, nf + 144])
+    K, it, st = eqd.stiffness_columns(fe, cols)
+    K64 = eqd.stiffness_columns(fe64, cols)[0]
+    assert (st == 1).all(), (st, it)
+    assert rel(K, K64) < K_TOL
