@@ -9,7 +9,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libeqd.so")
+# EQD_LIB selects another build of the library (e.g. a debug build).
+LIB_PATH = os.environ.get("EQD_LIB") or os.path.join(HERE, "lib", "libeqd.so")
 
 EQD_OK = 0
 EQD_ERR_ARG = 1

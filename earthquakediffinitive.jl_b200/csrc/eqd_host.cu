@@ -184,6 +184,7 @@ struct eqd_grid {
     MarchCfg m32, m64;
     int m64_maxt = 384;   // launch bound of the FP64 instance the grid runs
     bool served = false;  // attached to an eqd_server (its worker owns the grid)
+    int num_sms = 148;
     DevBuf dinv64, dinv32;   // Jacobi weights (one column, device layout)
     bool jacobi_ready = false;
     // FP32 A-apply launch variants (see make_variants) and the chosen one.
@@ -196,8 +197,10 @@ struct eqd_grid {
     int nchunks = 1;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;          // second half of a split batch (graph capture only)
+    cudaStream_t stream_hi = nullptr, stream2_hi = nullptr;  // high priority: vector kernels of the halves
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t evA = nullptr, evB = nullptr, evFork = nullptr, evJoin = nullptr;
+    cudaEvent_t evA = nullptr, evB = nullptr, evFork = nullptr, evJoin = nullptr, evArest = nullptr,
+                evBrest = nullptr;
     DevBuf err;           // device error word
     Workspace ws;
     std::mutex mtx;
@@ -457,11 +460,18 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
         // process: set it to the device maximum, once per device.
         CUDA_OR_RETURN(configure_kernels(optin));
     }
+    CUDA_OR_RETURN(cudaDeviceGetAttribute(&G->num_sms, cudaDevAttrMultiProcessorCount, d->device));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream2, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        CUDA_OR_RETURN(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream_hi, cudaStreamNonBlocking, greatest));
+        CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream2_hi, cudaStreamNonBlocking, greatest));
+    }
     CUDA_OR_RETURN(cudaEventCreate(&G->ev0));
     CUDA_OR_RETURN(cudaEventCreate(&G->ev1));
-    for (cudaEvent_t *e : {&G->evA, &G->evB, &G->evFork, &G->evJoin})
+    for (cudaEvent_t *e : {&G->evA, &G->evB, &G->evFork, &G->evJoin, &G->evArest, &G->evBrest})
         CUDA_OR_RETURN(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CUDA_OR_RETURN(G->err.ensure(sizeof(unsigned)));
     CUDA_OR_RETURN(cudaMemset(G->err.p, 0, sizeof(unsigned)));
@@ -479,9 +489,10 @@ extern "C" int eqd_grid_destroy(eqd_grid *G) {
     if (G->stream) cudaStreamSynchronize(G->stream);
     if (G->ev0) cudaEventDestroy(G->ev0);
     if (G->ev1) cudaEventDestroy(G->ev1);
-    for (cudaEvent_t e : {G->evA, G->evB, G->evFork, G->evJoin})
+    for (cudaEvent_t e : {G->evA, G->evB, G->evFork, G->evJoin, G->evArest, G->evBrest})
         if (e) cudaEventDestroy(e);
-    if (G->stream2) cudaStreamDestroy(G->stream2);
+    for (cudaStream_t t : {G->stream2, G->stream_hi, G->stream2_hi})
+        if (t) cudaStreamDestroy(t);
     if (G->stream) cudaStreamDestroy(G->stream);
     delete G;
     return EQD_OK;
@@ -643,6 +654,7 @@ static int resolve_chunk(eqd_grid *G, const eqd_solve_opts &o, int ncols, int pr
 struct Span {
     int c0, n;
     cudaStream_t s;
+    bool split;  // one of two halves whose kernels overlap
 };
 
 template <typename T>
@@ -688,6 +700,16 @@ static void record_apply(eqd_grid *G, Workspace &W, int generic, const SolvePara
         launch_march<T, T, MODE_A>(G, P.p, P.q, P.cs, P.apply_part, sn.n, -1, sn.s);
 }
 
+// CTA size of the vector kernels inside the iterations: small enough
+// (128 threads x 32 registers) to fit beside two resident stencil CTAs on an
+// SM, so the other half's updates can run while an apply is in flight.
+static constexpr int kVecThreads = 128;
+// With a split batch the vector kernels run on 4 CTAs per SM (grid-stride):
+// they fit beside the other half's stencil CTAs and still stream at close to
+// HBM speed (measured at h = 50 m: 1, 2, 4, 8 CTAs per SM and one CTA per item
+// gave 6.0, 6.6, 6.5, 6.3 k columns/s; one chain with one CTA per item 6.2 k).
+static constexpr int kVecCtasPerSm = 4;
+
 // The rest of the iteration: x, r updates; scalars; reliable update (mixed);
 // the next direction.
 template <typename T>
@@ -697,20 +719,23 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
     const int nch = G->nchunks;
     const double *dinv64 = sp.precond ? G->dinv64.as<double>() : nullptr;
     const float *dinv32 = sp.precond ? G->dinv32.as<float>() : nullptr;
-    const unsigned nb = (unsigned)(sn.n * nch);
+    // Split: a few CTAs per SM (grid-stride over the items) so they fit
+    // beside the other half's stencil CTAs; one chain: one CTA per item.
+    const long long items = (long long)sn.n * nch;
+    const unsigned nb = (unsigned)(sn.split ? std::min<long long>(items, (long long)G->num_sms * kVecCtasPerSm) : items);
     if (mixed) {
-        cg_update_kernel<float, float><<<nb, 256, 0, sn.s>>>(P.d, (float *)P.r, (const float *)P.p,
+        cg_update_kernel<float, float><<<nb, kVecThreads, 0, sn.s>>>(P.d, (float *)P.r, (const float *)P.p,
                                                             (const float *)P.q, P.apply_part, P.st, sp, P.rr_part,
-                                                            dinv32);
+                                                            dinv32, sn.n);
     } else {
-        cg_update_kernel<double, double><<<nb, 256, 0, sn.s>>>(P.x64, (double *)P.r, (const double *)P.p,
+        cg_update_kernel<double, double><<<nb, kVecThreads, 0, sn.s>>>(P.x64, (double *)P.r, (const double *)P.p,
                                                               (const double *)P.q, P.apply_part, P.st, sp,
-                                                              P.rr_part, dinv64);
+                                                              P.rr_part, dinv64, sn.n);
     }
     const unsigned sb = (unsigned)((sn.n + 127) / 128);
     cg_scalar_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp, P.apply_part, P.rr_part, sn.n, mixed);
     if (mixed) {
-        fold_correction_kernel<<<nb, 256, 0, sn.s>>>(P.x64, P.d, P.st, sp);
+        fold_correction_kernel<<<nb, kVecThreads, 0, sn.s>>>(P.x64, P.d, P.st, sp, sn.n);
         ColumnSet cf = P.cs;
         cf.flag = P.st.flag;
         cf.dinv = dinv64;
@@ -720,7 +745,7 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
         cg_true_residual_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp2, P.res_part, sn.n, 1);
     }
     const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
-    cg_pupdate_kernel<T><<<nb, 256, 0, sn.s>>>(P.p, P.r, P.st, sp, nullptr, dinvT);
+    cg_pupdate_kernel<T><<<nb, kVecThreads, 0, sn.s>>>(P.p, P.r, P.st, sp, nullptr, dinvT, sn.n);
 }
 
 // Capture kIter CG iterations over `cap` slots. Large batches are split in
@@ -731,29 +756,43 @@ template <typename T>
 static void record_iterations(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, const SolveParams &sp,
                               const ColState &st, int kIter, bool split) {
     if (!split) {
-        const Span all{0, cap, G->stream};
+        const Span all{0, cap, G->stream, false};
         for (int k = 0; k < kIter; ++k) {
             record_apply<T>(G, W, generic, sp, st, all);
             record_rest<T>(G, W, mixed, sp, st, all);
         }
         return;
     }
+    // Applies on normal-priority streams, the rest of each iteration on
+    // high-priority streams (node priorities are kept at instantiation), so
+    // that freed SM slots go to the short memory-bound kernels first.
     const int h0 = cap / 2;
-    const Span A{0, h0, G->stream}, B{h0, cap - h0, G->stream2};
+    const Span A{0, h0, G->stream, true}, B{h0, cap - h0, G->stream2, true};
+    const Span Ah{0, h0, G->stream_hi, true}, Bh{h0, cap - h0, G->stream2_hi, true};
     cudaEventRecord(G->evFork, A.s);
-    cudaStreamWaitEvent(B.s, G->evFork, 0);
+    for (cudaStream_t t : {B.s, Ah.s, Bh.s}) cudaStreamWaitEvent(t, G->evFork, 0);
     for (int k = 0; k < kIter; ++k) {
-        if (k > 0) cudaStreamWaitEvent(A.s, G->evB, 0);  // B's previous apply is done
+        if (k > 0) {
+            cudaStreamWaitEvent(A.s, G->evB, 0);      // B's previous apply is done
+            cudaStreamWaitEvent(A.s, G->evArest, 0);  // A's previous direction is ready
+        }
         record_apply<T>(G, W, generic, sp, st, A);
         cudaEventRecord(G->evA, A.s);
-        cudaStreamWaitEvent(B.s, G->evA, 0);             // B's apply follows A's
+        cudaStreamWaitEvent(B.s, G->evA, 0);          // B's apply follows A's
+        if (k > 0) cudaStreamWaitEvent(B.s, G->evBrest, 0);
         record_apply<T>(G, W, generic, sp, st, B);
         cudaEventRecord(G->evB, B.s);
-        record_rest<T>(G, W, mixed, sp, st, A);
-        record_rest<T>(G, W, mixed, sp, st, B);
+        cudaStreamWaitEvent(Ah.s, G->evA, 0);
+        record_rest<T>(G, W, mixed, sp, st, Ah);
+        cudaEventRecord(G->evArest, Ah.s);
+        cudaStreamWaitEvent(Bh.s, G->evB, 0);
+        record_rest<T>(G, W, mixed, sp, st, Bh);
+        cudaEventRecord(G->evBrest, Bh.s);
     }
     cudaEventRecord(G->evJoin, B.s);
     cudaStreamWaitEvent(A.s, G->evJoin, 0);
+    cudaStreamWaitEvent(A.s, G->evArest, 0);
+    cudaStreamWaitEvent(A.s, G->evBrest, 0);
 }
 
 // Jacobi weights dinv = 1 / diag(A) (zeros floored to 1), computed once per
@@ -948,7 +987,7 @@ struct SlotRun {
             record_iterations<T>(G, w, cap, mixed, generic, sp, st, kIter, split);
             cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-            ce = cudaGraphInstantiate(&w.graph, g, 0);
+            ce = cudaGraphInstantiate(&w.graph, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
             w.graph_key = kv;
@@ -1046,7 +1085,7 @@ struct SlotRun {
         }
         const T *dinvT = !sp.precond ? nullptr
                                      : (const T *)(sizeof(T) == 4 ? (const void *)G->dinv32.p : (const void *)G->dinv64.p);
-        cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), w.v0.as<T>(), st, sp, mask, dinvT);
+        cg_pupdate_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), w.v0.as<T>(), st, sp, mask, dinvT, cap);
         ++launches;
         CUDA_OR_RETURN(cudaGetLastError());
         return EQD_OK;
@@ -1617,11 +1656,10 @@ extern "C" int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_d
 
 // ---------------------------------------------------------------------------
 // Server: continuous batching of stiffness-column requests across grids.
-// One worker thread drives every attached grid's slot engine: it admits
-// queued columns into free slots, starts each grid's next graph of
-// iterations (grids on their own streams, so their work overlaps on the
-// device), then collects finished columns and writes them to their
-// requests' host buffers.
+// Each attached grid has a slot engine and a worker thread of its own: it
+// admits queued columns into free slots, runs the next graph of iterations
+// on the grid's streams (grids overlap on the device), then collects
+// finished columns and writes them to their requests' host buffers.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1645,7 +1683,7 @@ struct SrvGrid {
     std::deque<ColWork> pending;  // guarded by the server mutex
     PinnedArr<double> kstage;     // finished K columns, compact
     std::vector<ColDone> done;
-    bool launched = false;
+    std::thread worker;
     int held() const { return r32 ? r32->held : r64->held; }
     int free_slots() const { return r32 ? r32->free_slots() : r64->free_slots(); }
 };
@@ -1662,8 +1700,7 @@ struct eqd_server {
     std::map<int64_t, std::unique_ptr<SrvRequest>> reqs;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::thread worker;
-    bool stop = false, started = false;
+    bool stop = false;
     int64_t next_id = 1;
     int fatal = EQD_OK;
     std::string fatal_msg;
@@ -1688,100 +1725,86 @@ static void server_fail_all(eqd_server *S, int code, const std::string &msg) {
     S->cv_done.notify_all();
 }
 
-// One pass of the worker over every grid. Returns an error code.
-static int server_pass(eqd_server *S) {
-    // Phase 1: admit queued columns and start each busy grid's iterations.
-    for (auto &gp : S->grids) {
-        SrvGrid &g = *gp;
-        g.launched = false;
-        std::vector<ColWork> take;
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            const int nfree = g.free_slots();
-            while ((int)take.size() < nfree && !g.pending.empty()) {
-                take.push_back(g.pending.front());
-                g.pending.pop_front();
-            }
-            const double t = S->now();
-            for (const ColWork &c : take) {
-                auto it = S->reqs.find(c.tag >> kTagBits);
-                if (it != S->reqs.end() && it->second->state == 0) {
-                    it->second->state = 1;
-                    it->second->t_start = t;
-                }
-            }
+// One pass of a grid's worker: admit queued columns into free slots, run
+// the next graph of iterations, deliver the columns that finished.
+static int grid_pass(eqd_server *S, SrvGrid &g) {
+    eqd_grid *G = g.G;
+    std::vector<ColWork> take;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        const int nfree = g.free_slots();
+        while ((int)take.size() < nfree && !g.pending.empty()) {
+            take.push_back(g.pending.front());
+            g.pending.pop_front();
         }
-        if (cudaSetDevice(g.G->desc.device) != cudaSuccess) return fail(EQD_ERR_CUDA, "cudaSetDevice failed");
-        int rc = EQD_OK, taken = 0;
-        if (!take.empty())
-            rc = g.r32 ? g.r32->admit(take.data(), (int)take.size(), taken)
-                       : g.r64->admit(take.data(), (int)take.size(), taken);
-        if (rc) return rc;
-        if (g.held() > 0) {
-            rc = g.r32 ? g.r32->launch() : g.r64->launch();
-            if (rc) return rc;
-            g.launched = true;
+        const double t = S->now();
+        for (const ColWork &c : take) {
+            auto it = S->reqs.find(c.tag >> kTagBits);
+            if (it != S->reqs.end() && it->second->state == 0) {
+                it->second->state = 1;
+                it->second->t_start = t;
+            }
         }
     }
-    // Phase 2: collect finished columns, extract their K columns, deliver.
-    for (auto &gp : S->grids) {
-        SrvGrid &g = *gp;
-        if (!g.launched) continue;
-        eqd_grid *G = g.G;
-        if (cudaSetDevice(G->desc.device) != cudaSuccess) return fail(EQD_ERR_CUDA, "cudaSetDevice failed");
-        int rc = g.r32 ? g.r32->collect(g.done) : g.r64->collect(g.done);
-        if (rc) return rc;
-        if (g.done.empty()) continue;
-        const int nf2 = 2 * G->gc.nf;
-        rc = g.r32 ? g.r32->extract(g.done, G->ws.kout.as<double>(), nf2, false)
-                   : g.r64->extract(g.done, G->ws.kout.as<double>(), nf2, false);
-        if (rc) return rc;
-        CUDA_OR_RETURN(cudaMemcpyAsync(g.kstage.data(), G->ws.kout.p, sizeof(double) * nf2 * g.done.size(),
-                                       cudaMemcpyDeviceToHost, G->stream));
-        CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            const double t = S->now();
-            bool any_done = false;
-            for (size_t j = 0; j < g.done.size(); ++j) {
-                const ColDone &d = g.done[j];
-                auto it = S->reqs.find(d.tag >> kTagBits);
-                if (it == S->reqs.end()) continue;
-                SrvRequest &r = *it->second;
-                const long long pos = d.tag & ((1LL << kTagBits) - 1);
-                std::memcpy(r.k_out + (size_t)pos * nf2, g.kstage.data() + j * nf2, sizeof(double) * nf2);
-                r.iterations += d.iters;
-                r.max_it = std::max(r.max_it, d.iters);
-                if (d.status != COL_CONVERGED) ++r.unconverged;
-                if (--r.remaining == 0) {
-                    r.state = 2;
-                    r.t_done = t;
-                    any_done = true;
-                }
+    int rc = EQD_OK, taken = 0;
+    if (!take.empty())
+        rc = g.r32 ? g.r32->admit(take.data(), (int)take.size(), taken)
+                   : g.r64->admit(take.data(), (int)take.size(), taken);
+    if (rc) return rc;
+    if (g.held() == 0) return EQD_OK;
+    rc = g.r32 ? g.r32->advance(g.done) : g.r64->advance(g.done);
+    if (rc) return rc;
+    if (g.done.empty()) return EQD_OK;
+    const int nf2 = 2 * G->gc.nf;
+    rc = g.r32 ? g.r32->extract(g.done, G->ws.kout.as<double>(), nf2, false)
+               : g.r64->extract(g.done, G->ws.kout.as<double>(), nf2, false);
+    if (rc) return rc;
+    CUDA_OR_RETURN(cudaMemcpyAsync(g.kstage.data(), G->ws.kout.p, sizeof(double) * nf2 * g.done.size(),
+                                   cudaMemcpyDeviceToHost, G->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        const double t = S->now();
+        bool any_done = false;
+        for (size_t j = 0; j < g.done.size(); ++j) {
+            const ColDone &d = g.done[j];
+            auto it = S->reqs.find(d.tag >> kTagBits);
+            if (it == S->reqs.end()) continue;
+            SrvRequest &r = *it->second;
+            const long long pos = d.tag & ((1LL << kTagBits) - 1);
+            std::memcpy(r.k_out + (size_t)pos * nf2, g.kstage.data() + j * nf2, sizeof(double) * nf2);
+            r.iterations += d.iters;
+            r.max_it = std::max(r.max_it, d.iters);
+            if (d.status != COL_CONVERGED) ++r.unconverged;
+            if (--r.remaining == 0) {
+                r.state = 2;
+                r.t_done = t;
+                any_done = true;
             }
-            if (any_done) S->cv_done.notify_all();
         }
-        rc = g.r32 ? g.r32->release(g.done) : g.r64->release(g.done);
-        if (rc) return rc;
+        if (any_done) S->cv_done.notify_all();
     }
-    return EQD_OK;
+    return g.r32 ? g.r32->release(g.done) : g.r64->release(g.done);
 }
 
-static void server_loop(eqd_server *S) {
+// One worker thread per grid: a grid advances at its own pace (its graphs
+// run on its own streams), so a request on a small grid is not held behind
+// the long iterations of a large one.
+static void grid_loop(eqd_server *S, SrvGrid *g) {
+    if (cudaSetDevice(g->G->desc.device) != cudaSuccess) {
+        server_fail_all(S, EQD_ERR_CUDA, "cudaSetDevice failed in a server worker");
+        return;
+    }
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] {
-                if (S->stop) return true;
-                for (auto &g : S->grids)
-                    if (!g->pending.empty() || g->held() > 0) return true;
-                return false;
-            });
-            if (S->stop) return;
+            S->cv_work.wait(lk, [&] { return S->stop || S->fatal || !g->pending.empty() || g->held() > 0; });
+            if (S->stop || S->fatal) return;
         }
-        const int rc = server_pass(S);
+        const int rc = grid_pass(S, *g);
         if (rc) {
             server_fail_all(S, rc, g_last_error);
+            S->cv_work.notify_all();
             return;
         }
     }
@@ -1806,6 +1829,29 @@ extern "C" int eqd_server_create(const eqd_solve_opts *opts, uint64_t hbm_budget
         S->budget = fr > keep ? fr - keep : fr / 2;
     }
     *out = S.release();
+    return EQD_OK;
+}
+
+// Stream priorities of a served grid: smaller grids get higher priority, so
+// their short kernels take SM slots ahead of a large grid's long ones (a
+// request on the h = 100 m grid is not starved by h = 25 m work). Within a
+// grid the vector kernels stay one level above the stencil applies.
+static int set_grid_priority(eqd_grid *G) {
+    int least = 0, greatest = 0;
+    CUDA_OR_RETURN(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const double ntot = 6.0 * G->gc.n1 * G->gc.n2 * G->gc.n3;
+    const int bucket = std::max(0, (int)std::floor(std::log10(std::max(ntot, 1.0))) - 4);  // 0: < 1e5 DOF
+    const int step = least > greatest ? -1 : 1;                 // direction of "higher priority"
+    const int span = std::abs(least - greatest);
+    const int main_p = greatest - step * std::min(span, 1 + bucket);
+    const int rest_p = greatest - step * std::min(span, bucket);
+    CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
+    for (cudaStream_t t : {G->stream, G->stream2, G->stream_hi, G->stream2_hi}) cudaStreamDestroy(t);
+    CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream, cudaStreamNonBlocking, main_p));
+    CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream2, cudaStreamNonBlocking, main_p));
+    CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream_hi, cudaStreamNonBlocking, rest_p));
+    CUDA_OR_RETURN(cudaStreamCreateWithPriority(&G->stream2_hi, cudaStreamNonBlocking, rest_p));
+    G->ws.graph_key.clear();  // recapture on the new streams
     return EQD_OK;
 }
 
@@ -1836,7 +1882,12 @@ extern "C" int eqd_server_add_grid(eqd_server *S, eqd_grid *G, int32_t slots) {
         S->used += g->bytes;
     }
     g->G = G;
-    int rc;
+    int rc = set_grid_priority(G);
+    if (rc) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->used -= g->bytes;
+        return rc;
+    }
     if (mixed) {
         g->r32.reset(new SlotRun<float>());
         rc = g->r32->setup(G, S->opts, g->slots, false, false);
@@ -1859,11 +1910,9 @@ extern "C" int eqd_server_add_grid(eqd_server *S, eqd_grid *G, int32_t slots) {
     }
     G->served = true;
     std::lock_guard<std::mutex> lk(S->mu);
+    SrvGrid *gp = g.get();
     S->grids.push_back(std::move(g));
-    if (!S->started) {
-        S->started = true;
-        S->worker = std::thread(server_loop, S);
-    }
+    gp->worker = std::thread(grid_loop, S, gp);
     return EQD_OK;
 }
 
@@ -1899,7 +1948,7 @@ extern "C" int eqd_server_submit(eqd_server *S, eqd_grid *G, const int32_t *cols
     }
     *request_id = r->id;
     S->reqs[r->id] = std::move(r);
-    S->cv_work.notify_one();
+    S->cv_work.notify_all();
     return EQD_OK;
 }
 
@@ -1964,7 +2013,8 @@ extern "C" int eqd_server_destroy(eqd_server *S) {
         S->stop = true;
     }
     S->cv_work.notify_all();
-    if (S->worker.joinable()) S->worker.join();
+    for (auto &g : S->grids)
+        if (g->worker.joinable()) g->worker.join();
     for (auto &g : S->grids) {
         cudaSetDevice(g->G->desc.device);
         cudaStreamSynchronize(g->G->stream);

@@ -429,6 +429,13 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         c1[5] = T(0);
         c2[5] = T(0);
     }
+    // Face threads: the +x1 boundary derivative of the fault node over the
+    // same 6-wide x1 window (lower end of the plus block: window cols 0..3;
+    // upper end of the minus block: cols 5..2, odd mirror).
+    T cdh[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        cdh[k] = !is_face ? T(0) : (side == 1 ? (k < 4 ? A1.dlo[k] : T(0)) : (k >= 2 ? -A1.dlo[5 - k] : T(0)));
     const bool ff_x12 = (side == 0 && i1 == 0) || (side == 1 && i1 == n1 - 1) || i2 == 0 || i2 == n2 - 1;
     const T wq1 = (i1 < 4) ? A1.wq[i1] : (i1 >= n1 - 4 ? A1.wq[n1 - 1 - i1] : T(1));
     const T wq2 = (i2 < 4) ? A2.wq[i2] : (i2 >= n2 - 4 ? A2.wq[n2 - 1 - i2] : T(1));
@@ -563,13 +570,25 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 const T *o3 = o2 + CH;
                 const T v1 = v1w[l][3], v2 = v2w[l][3], v3 = v3w[l][3];
                 T G1 = T(0), A11 = T(0), A21 = T(0), A31 = T(0);
+                T xa[6], xb[6], xc[6];
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
-                    const T x1 = l1[k], x2 = l2[k], x3 = l3[k];
-                    G1 += c1[k] * x1;
-                    A11 += c2[k] * x1;
-                    A21 += c2[k] * x2;
-                    A31 += c2[k] * x3;
+                    xa[k] = l1[k];
+                    xb[k] = l2[k];
+                    xc[k] = l3[k];
+                    G1 += c1[k] * xa[k];
+                    A11 += c2[k] * xa[k];
+                    A21 += c2[k] * xb[k];
+                    A31 += c2[k] * xc[k];
+                }
+                T dh1 = T(0), dh2 = T(0), dh3 = T(0);
+                if (is_face) {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        dh1 += cdh[k] * xa[k];
+                        dh2 += cdh[k] * xb[k];
+                        dh3 += cdh[k] * xc[k];
+                    }
                 }
                 T G2 = x2_d1i(A2, o2, n1);
                 T H21 = x2_d1i(A2, o1, n1);
@@ -605,19 +624,9 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                 w3p[l] = mu * (A31 + A32 + T(2) * A33);
                 if (is_face) {
                     // Traction on the fixed +x1 axis (`traction_blocks`), with the
-                    // +x1 boundary derivative of the fault node: lower end of the
-                    // plus block (window cols 0..3), upper end of the minus block
-                    // (window cols 5..2, odd mirror). SAT c (tau^+ - tau^-) on both
-                    // faces; the partner (other side) is the adjacent lane.
-                    T dh1 = T(0), dh2 = T(0), dh3 = T(0);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int q = side == 1 ? k : 5 - k;
-                        const T cf = side == 1 ? A1.dlo[k] : -A1.dlo[k];
-                        dh1 += cf * l1[q];
-                        dh2 += cf * l2[q];
-                        dh3 += cf * l3[q];
-                    }
+                    // +x1 boundary derivatives dh (computed with the x1 window).
+                    // SAT c (tau^+ - tau^-) on both faces; the partner (other
+                    // side) is the adjacent lane.
                     const T D3v1 = x3i ? x3_d1i(A3, v1w[l]) : x3_d1c(A3, v1w[l], r3);
                     const T tau1 = lam * (G1 + G2 + G3) + T(2) * mu * dh1;
                     const T tau2 = mu * (H21 + dh2);

@@ -39,51 +39,81 @@ struct SolveParams {
 // ---------------------------------------------------------------------------
 // rr_part[col][chunk][2] = (r.r, r.z) partials; r.z = r.r without a
 // preconditioner (`dinv` null), z = dinv r with one (Jacobi).
+// Grid-stride over (column, chunk) items: any grid size gives the same
+// per-item partial sums, so a small grid (a few CTAs per SM, able to run
+// beside the stencil apply) is as exact as one CTA per item.
 template <typename T, typename TX>
 __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *__restrict__ r,
                                                         const T *__restrict__ p, const T *__restrict__ q,
                                                         const double *__restrict__ apply_part, ColState st,
                                                         SolveParams sp, double *__restrict__ rr_part,
-                                                        const T *__restrict__ dinv = nullptr) {
-    const int col = blockIdx.x / sp.nchunks;
-    const int chunk = blockIdx.x % sp.nchunks;
-    if (st.status[col] != COL_ACTIVE) return;
+                                                        const T *__restrict__ dinv, int ncols) {
     __shared__ double red[32];
     __shared__ double s_alpha;
-    if (threadIdx.x == 0) {
-        double pq = 0.0, pp = 0.0;
-        for (int t = 0; t < sp.ntiles; ++t) {
-            pq += apply_part[((long long)col * sp.ntiles + t) * 2 + 0];
-            pp += apply_part[((long long)col * sp.ntiles + t) * 2 + 1];
+    const int nitems = ncols * sp.nchunks;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int col = item / sp.nchunks;
+        const int chunk = item % sp.nchunks;
+        if (st.status[col] != COL_ACTIVE) continue;
+        if (threadIdx.x == 0) {
+            double pq = 0.0, pp = 0.0;
+            for (int t = 0; t < sp.ntiles; ++t) {
+                pq += apply_part[((long long)col * sp.ntiles + t) * 2 + 0];
+                pp += apply_part[((long long)col * sp.ntiles + t) * 2 + 1];
+            }
+            double a = st.gamma[col] / pq;
+            if (!(pq > 2.220446049250313e-16 * pp) || !isfinite(a)) a = 0.0;  // breakdown: scalar kernel flags it
+            s_alpha = a;
         }
-        double a = st.gamma[col] / pq;
-        if (!(pq > 2.220446049250313e-16 * pp) || !isfinite(a)) a = 0.0;  // breakdown: scalar kernel flags it
-        s_alpha = a;
-    }
-    __syncthreads();
-    const double alpha = s_alpha;
-    const long long n = sp.colstride;
-    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
-    const long long off = (long long)col * n;
-    double acc = 0.0, accz = 0.0;
-    const T a_t = (T)alpha;
-    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
-        const T pi = p[off + i], qi = q[off + i];
-        x[off + i] = (TX)(x[off + i] + (TX)alpha * (TX)pi);
-        const T ri = r[off + i] - a_t * qi;
-        r[off + i] = ri;
-        acc += (double)ri * (double)ri;
-        if (dinv) accz += (double)dinv[i] * (double)ri * (double)ri;
-    }
-    const double s = block_sum(acc, red);
-    double sz = s;
-    if (dinv) {
         __syncthreads();
-        sz = block_sum(accz, red);
-    }
-    if (threadIdx.x == 0) {
-        rr_part[((long long)col * sp.nchunks + chunk) * 2 + 0] = s;
-        rr_part[((long long)col * sp.nchunks + chunk) * 2 + 1] = sz;
+        const double alpha = s_alpha;
+        const long long n = sp.colstride;
+        const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+        const long long off = (long long)col * n;
+        double acc = 0.0, accz = 0.0;
+        const T a_t = (T)alpha;
+        // Four independent elements per thread per pass: enough loads in
+        // flight for HBM speed with few CTAs per SM.
+        const long long bd = blockDim.x;
+        long long i = beg + threadIdx.x;
+        for (; i + 3 * bd < end; i += 4 * bd) {
+            T pi[4], qi[4], ri[4];
+            TX xi[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                pi[u] = p[off + i + u * bd];
+                qi[u] = q[off + i + u * bd];
+                ri[u] = r[off + i + u * bd];
+                xi[u] = x[off + i + u * bd];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                x[off + i + u * bd] = (TX)(xi[u] + (TX)alpha * (TX)pi[u]);
+                const T rn = ri[u] - a_t * qi[u];
+                r[off + i + u * bd] = rn;
+                acc += (double)rn * (double)rn;
+                if (dinv) accz += (double)dinv[i + u * bd] * (double)rn * (double)rn;
+            }
+        }
+        for (; i < end; i += bd) {
+            const T pi = p[off + i], qi = q[off + i];
+            x[off + i] = (TX)(x[off + i] + (TX)alpha * (TX)pi);
+            const T ri = r[off + i] - a_t * qi;
+            r[off + i] = ri;
+            acc += (double)ri * (double)ri;
+            if (dinv) accz += (double)dinv[i] * (double)ri * (double)ri;
+        }
+        const double s = block_sum(acc, red);
+        double sz = s;
+        if (dinv) {
+            __syncthreads();
+            sz = block_sum(accz, red);
+        }
+        if (threadIdx.x == 0) {
+            rr_part[((long long)col * sp.nchunks + chunk) * 2 + 0] = s;
+            rr_part[((long long)col * sp.nchunks + chunk) * 2 + 1] = sz;
+        }
+        __syncthreads();
     }
 }
 
@@ -92,36 +122,50 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
 // With a preconditioner: p = dinv r + beta p.
 template <typename T>
 __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, const T *__restrict__ r, ColState st,
-                                                         SolveParams sp, const int8_t *__restrict__ mask = nullptr,
-                                                         const T *__restrict__ dinv = nullptr) {
-    const int col = blockIdx.x / sp.nchunks;
-    const int chunk = blockIdx.x % sp.nchunks;
-    if (st.status[col] != COL_ACTIVE) return;
-    if (mask && !mask[col]) return;
-    const T b = (T)st.beta[col];
-    const long long n = sp.colstride;
-    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
-    const long long off = (long long)col * n;
-    if (dinv) {
-        for (long long i = beg + threadIdx.x; i < end; i += blockDim.x)
-            p[off + i] = dinv[i] * r[off + i] + b * p[off + i];
-    } else {
-        for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) p[off + i] = r[off + i] + b * p[off + i];
+                                                         SolveParams sp, const int8_t *__restrict__ mask,
+                                                         const T *__restrict__ dinv, int ncols) {
+    const int nitems = ncols * sp.nchunks;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int col = item / sp.nchunks;
+        const int chunk = item % sp.nchunks;
+        if (st.status[col] != COL_ACTIVE) continue;
+        if (mask && !mask[col]) continue;
+        const T b = (T)st.beta[col];
+        const long long n = sp.colstride;
+        const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+        const long long off = (long long)col * n;
+        const long long bd = blockDim.x;
+        long long i = beg + threadIdx.x;
+        for (; i + 3 * bd < end; i += 4 * bd) {
+            T ri[4], pi[4], zi[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                ri[u] = r[off + i + u * bd];
+                pi[u] = p[off + i + u * bd];
+                zi[u] = dinv ? dinv[i + u * bd] : T(1);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) p[off + i + u * bd] = (dinv ? zi[u] * ri[u] : ri[u]) + b * pi[u];
+        }
+        for (; i < end; i += bd) p[off + i] = (dinv ? dinv[i] * r[off + i] : r[off + i]) + b * p[off + i];
     }
 }
 
 // Mixed precision: fold the FP32 correction into the FP64 solution.
 __global__ void __launch_bounds__(256) fold_correction_kernel(double *__restrict__ x, float *__restrict__ d, ColState st,
-                                                              SolveParams sp) {
-    const int col = blockIdx.x / sp.nchunks;
-    const int chunk = blockIdx.x % sp.nchunks;
-    if (st.status[col] != COL_ACTIVE || !st.flag[col]) return;
-    const long long n = sp.colstride;
-    const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
-    const long long off = (long long)col * n;
-    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
-        x[off + i] += (double)d[off + i];
-        d[off + i] = 0.f;
+                                                              SolveParams sp, int ncols) {
+    const int nitems = ncols * sp.nchunks;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int col = item / sp.nchunks;
+        const int chunk = item % sp.nchunks;
+        if (st.status[col] != COL_ACTIVE || !st.flag[col]) continue;
+        const long long n = sp.colstride;
+        const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
+        const long long off = (long long)col * n;
+        for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
+            x[off + i] += (double)d[off + i];
+            d[off + i] = 0.f;
+        }
     }
 }
 
