@@ -307,7 +307,7 @@ def main():
     eqd._abi.check(lib.eqd_autotune(fe.handle, C.c_int32(min(len(cols), 512)), C.byref(sel), tms, trows, tthr,
                                     C.byref(nv)))
     autotune = {"selected": sel.value,
-                "variants": [{"tile_rows": trows[i], "threads": tthr[i], "ms_512_columns": tms[i]}
+                "variants": [{"tile_rows": trows[i], "threads": tthr[i], "ms_per_cg_iteration": tms[i]}
                              for i in range(nv.value)]}
 
     # Roofline of the dominant kernel: FP32 stencil apply over the batch.

@@ -76,7 +76,7 @@ static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register s
 static constexpr int kMaxT32c = 384;  // FP32 A-apply, two columns per thread
 static constexpr int kMaxT64 = 384;
 static constexpr int kMaxT64b = 512;  // FP64 instances for wide x1 lines (n1 = 33 needs 7 x 66 threads)
-static constexpr int kNumVariants = 5;
+static constexpr int kNumVariants = 7;
 
 static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
 
@@ -85,7 +85,8 @@ static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
 // the n1-specialized instances).
 template <typename T>
 static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, int maxt, int tile_rows,
-                           const GridConst &gc, MarchCfg &out, std::string &why, int lanes = 1, int kmaxt = 0) {
+                           const GridConst &gc, MarchCfg &out, std::string &why, int lanes = 1, int kmaxt = 0,
+                           bool edge_mode = false) {
     if (kmaxt == 0) kmaxt = maxt;
     const int per_row = 2 * n1;
     int t2 = tile_rows > 0 ? std::min(tile_rows, maxt / per_row) : maxt / per_row;
@@ -98,7 +99,10 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     while (ntiles > 1 && n2 / ntiles < 7) --ntiles;
     int t2max = (n2 + ntiles - 1) / ntiles;
     int edge = 0;
-    if (t2max * per_row > maxt && t2 >= 7 && n2 >= 14) {
+    // Edge partition: forced (a launch variant that keeps every x2 closure row
+    // in 7-row edge tiles, so no CTA mixes closure and interior rows), or
+    // needed when balanced tiles of >= 7 rows do not fit the thread limit.
+    if ((edge_mode || t2max * per_row > maxt) && t2 >= 7 && n2 >= 14) {
         // Tiles of at most t2 rows: 7-row tiles at both ends carry the closure
         // rows, the tiles between (any height) split the interior.
         edge = 7;
@@ -427,18 +431,22 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
             return fail(EQD_ERR_ARG, why);
     }
     // FP32 A-apply variants: one large CTA per SM (640-thread bound, may
-    // spill), one CTA of up to 512 threads (no spill), and CTAs of up to 256
-    // threads so that two share an SM.
+    // spill), one CTA of up to 512 threads (no spill), CTAs of up to 256
+    // threads so that two share an SM, two columns per thread, and small
+    // edge-partitioned tiles (closure rows and interior rows in different CTAs).
     {
-        // thread limit, kernel launch bound, columns per thread
-        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192};
-        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c};
-        const int ln[kNumVariants] = {1, 1, 1, 2, 2};
+        // thread limit, kernel launch bound, columns per thread, tile rows
+        // (0: as many as fit), edge partition
+        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192, kMaxT32b, kMaxT32b};
+        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c, kMaxT32b, kMaxT32b};
+        const int ln[kNumVariants] = {1, 1, 1, 2, 2, 1, 1};
+        const int rows[kNumVariants] = {0, 0, 0, 0, 0, 7, 10};
+        const bool edg[kNumVariants] = {false, false, false, false, false, true, true};
         for (int v = 0; v < kNumVariants; ++v) {
             G->v32_maxt[v] = mt[v];
             G->v32_lanes[v] = ln[v];
-            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], 0, gc, G->v32[v], why,
-                                       ln[v], mt[v])) {
+            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], rows[v], gc, G->v32[v],
+                                       why, ln[v], mt[v], edg[v])) {
                 G->v32[v] = G->m32;  // fall back to the generic configuration
                 G->v32_maxt[v] = kMaxT32;
                 G->v32_lanes[v] = 1;
@@ -578,42 +586,6 @@ extern "C" int eqd_apply(eqd_grid *G, const double *x, double *y, int32_t ncols,
 // choice is fixed for the grid's lifetime, so every column of every later
 // call uses the same tile partition (and the same reduction order).
 // ---------------------------------------------------------------------------
-static int tune_variants(eqd_grid *G, int ncols) {
-    const GridConst &gc = G->gc;
-    ncols = std::max(ncols, 1);
-    DevBuf x, y, part;
-    const long long n = gc.colstride * (long long)ncols;
-    CUDA_OR_RETURN(x.ensure(sizeof(float) * n));
-    CUDA_OR_RETURN(y.ensure(sizeof(float) * n));
-    int ntmax = 1;
-    for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
-    CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * ntmax));
-    fill_random_kernel<float><<<1184, 256, 0, G->stream>>>(x.as<float>(), n, 777ull);
-    CUDA_OR_RETURN(cudaGetLastError());
-    ColumnSet cs{};
-    double best = 1e30;
-    int bestv = G->sel32;
-    for (int v = 0; v < kNumVariants; ++v) {
-        CUDA_OR_RETURN((launch_march<float, float, MODE_A>(G, x.as<float>(), y.as<float>(), cs, part.as<double>(),
-                                                            ncols, v)));
-        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
-        for (int r = 0; r < 3; ++r)
-            CUDA_OR_RETURN((launch_march<float, float, MODE_A>(G, x.as<float>(), y.as<float>(), cs,
-                                                                part.as<double>(), ncols, v)));
-        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
-        CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
-        float ms = 0.f;
-        CUDA_OR_RETURN(cudaEventElapsedTime(&ms, G->ev0, G->ev1));
-        G->tune_ms[v] = ms / 3.0;
-        if (G->tune_ms[v] < best) {
-            best = G->tune_ms[v];
-            bestv = v;
-        }
-    }
-    G->sel32 = bestv;
-    G->tuned = true;
-    return check_device_error(G);
-}
 
 // ---------------------------------------------------------------------------
 // Batched CG driver
@@ -844,6 +816,8 @@ struct ColDone {
     int8_t status;
 };
 
+static int tune_by_iterations(eqd_grid *G, const eqd_solve_opts &o, int ncols);
+
 // Page-locked host array: device-to-host copies into it stay asynchronous.
 template <typename E>
 struct PinnedArr {
@@ -900,7 +874,7 @@ struct SlotRun {
         const long long ntot = 6LL * gc.n1 * gc.n2 * gc.n3;
         const size_t vec = (size_t)gc.colstride * cap;
         if (mixed && !G->tuned) {
-            int rc = tune_variants(G, std::min(cap, 512));
+            int rc = tune_by_iterations(G, o, std::min(cap, 1024));
             if (rc) return rc;
         }
         const int nt32 = G->v32[G->sel32].g.ntiles, nt64 = G->m64.g.ntiles;
@@ -1184,6 +1158,53 @@ struct SlotRun {
     }
 };
 
+// Launch-variant tuner: time 20 CG iterations (two graph launches) of a
+// batch of `ncols` unit-slip columns with each FP32 stencil variant and keep
+// the fastest. The whole iteration is timed, not the stencil alone: a variant
+// that packs more stencil CTAs per SM can leave less room for the other
+// half's vector kernels (measured at h = 50 m: the fastest stencil alone was
+// not the fastest iteration).
+static int tune_by_iterations(eqd_grid *G, const eqd_solve_opts &o, int ncols) {
+    const GridConst &gc = G->gc;
+    ncols = std::max(1, std::min(ncols, 2 * gc.nf));
+    std::vector<ColWork> work(ncols);
+    for (int i = 0; i < ncols; ++i) {
+        work[i].slip_node = (int)(((long long)i * 7919 + gc.nf / 2) % gc.nf);
+        work[i].slip_comp = i & 1;
+        work[i].tag = i;
+    }
+    eqd_solve_opts ot = o;
+    ot.precision = EQD_PREC_MIXED;
+    G->tuned = true;  // the slot engines below must not tune again
+    double best = 1e30;
+    int bestv = G->sel32;
+    for (int v = 0; v < kNumVariants; ++v) {
+        G->sel32 = v;
+        SlotRun<float> R;
+        int rc = R.setup(G, ot, ncols, false, false);
+        if (rc) return rc;
+        int taken = 0;
+        rc = R.admit(work.data(), ncols, taken);
+        if (!rc) rc = R.launch();  // first launch: warm-up
+        if (rc) return rc;
+        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+        rc = R.launch();
+        if (!rc) rc = R.launch();
+        if (rc) return rc;
+        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+        CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
+        float ms = 0.f;
+        CUDA_OR_RETURN(cudaEventElapsedTime(&ms, G->ev0, G->ev1));
+        G->tune_ms[v] = ms / (2.0 * SlotRun<float>::kIter);
+        if (G->tune_ms[v] < best) {
+            best = G->tune_ms[v];
+            bestv = v;
+        }
+    }
+    G->sel32 = bestv;
+    return check_device_error(G);
+}
+
 // Batched solve through the slot engine: columns enter as slots free up; K
 // columns go to the caller's device or host buffer as each column finishes.
 template <typename T>
@@ -1445,7 +1466,9 @@ static int profile_apply_impl(eqd_grid *G, int ncols, int warmup, int reps, doub
     CUDA_OR_RETURN(x.ensure(sizeof(T) * n));
     CUDA_OR_RETURN(y.ensure(sizeof(T) * n));
     if (sizeof(T) == 4 && !G->tuned) {
-        int rc = tune_variants(G, std::min(ncols, 512));
+        eqd_solve_opts o;
+        eqd_default_opts(&o);
+        int rc = tune_by_iterations(G, o, std::min(ncols, 1024));
         if (rc) return rc;
     }
     int nt = G->m64.g.ntiles;
@@ -1485,7 +1508,9 @@ extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, doubl
     std::lock_guard<std::mutex> lk(G->mtx);
     if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
-    int rc = tune_variants(G, ncols);
+    eqd_solve_opts o;
+    eqd_default_opts(&o);
+    int rc = tune_by_iterations(G, o, ncols);
     if (rc) return rc;
     if (selected) *selected = G->sel32;
     if (nvariants) *nvariants = kNumVariants;
