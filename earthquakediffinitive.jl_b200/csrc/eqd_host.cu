@@ -707,7 +707,9 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
     const unsigned sb = (unsigned)((sn.n + 127) / 128);
     cg_scalar_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp, P.apply_part, P.rr_part, sn.n, mixed);
     if (mixed) {
-        fold_correction_kernel<<<nb, kVecThreads, 0, sn.s>>>(P.x64, P.d, P.st, sp, sn.n);
+        // One CTA per item: in most iterations no column is flagged and every
+        // CTA returns at once.
+        fold_correction_kernel<<<(unsigned)items, kVecThreads, 0, sn.s>>>(P.x64, P.d, P.st, sp, sn.n);
         ColumnSet cf = P.cs;
         cf.flag = P.st.flag;
         cf.dinv = dinv64;
