@@ -42,7 +42,8 @@ __all__ = [
     "elastic_solver_report", "frictional_node_count", "fault_grid_axes", "shear_traction",
     "fault_stiffness", "fault_stiffness_toeplitz", "stiffness_columns", "apply_operator",
     "KMatrix", "build_model", "EqdError", "EqdArgumentError", "library_path", "Server",
-    "operator_diagonal", "jacobi_preconditioner",
+    "operator_diagonal", "jacobi_preconditioner", "cached_fault_stiffness", "BP8Rhs", "FrictionParams",
+    "friction_solve",
 ]
 
 
@@ -452,3 +453,5 @@ def build_model(dz=50.0, L_fault=800.0, L_normal=400.0, l_f=400.0, mu=32.04e9, n
 
 
 from .serving import Server  # noqa: E402  (continuous-batching request server)
+from .kcache import cached_fault_stiffness  # noqa: E402  (on-disk K cache with resume)
+from .timeloop import BP8Rhs, FrictionParams, friction_solve  # noqa: E402  (time-loop RHS on the GPU)

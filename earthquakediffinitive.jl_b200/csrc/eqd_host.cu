@@ -19,6 +19,7 @@
 #include "../../include/eqd.h"
 #include "ops_tables.h"
 #include "solver_kernels.cuh"
+#include "rhs_kernels.cuh"
 
 using namespace eqd;
 
@@ -2051,5 +2052,212 @@ extern "C" int eqd_server_destroy(eqd_server *S) {
         g->G->served = false;
     }
     delete S;
+    return EQD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Time-loop right-hand side (eqd_rhs_*) and batched friction solves
+// ---------------------------------------------------------------------------
+struct eqd_rhs {
+    int device = 0;
+    int nf = 0;
+    int nslice = 1;
+    eqd_rhs_params p{};
+    DevBuf K, part, u, du, ap_ptr, ap_idx, ap_val, source, active, vprev, tau, sigma_low, floor_nodes, floor_hits,
+        status;
+    cudaStream_t stream = nullptr;
+};
+
+static FrictionConst friction_const(const eqd_rhs_params &p) {
+    return FrictionConst{p.a, p.b, p.Dc, p.V_star, p.f_star};
+}
+
+static bool newton_ok(const eqd_rhs_params &p) {
+    return p.newton_tol > 0 && p.newton_maxiter > 0 && p.newton_maxstep > 0 && p.a > 0 && p.Dc > 0 && p.V_star > 0;
+}
+
+extern "C" int eqd_rhs_create(int32_t device, int32_t nf, const double *K, const eqd_rhs_params *params,
+                              const int32_t *ap_ptr, const int32_t *ap_idx, const double *ap_val, const double *source,
+                              const uint8_t *active, eqd_rhs **out) {
+    if (!out || !K || !params || nf < 1 || !ap_ptr || (!ap_idx && ap_ptr[nf] > 0) || (!ap_val && ap_ptr[nf] > 0))
+        return fail(EQD_ERR_ARG, "invalid argument");
+    *out = nullptr;
+    if (!newton_ok(*params)) return fail(EQD_ERR_ARG, "invalid friction or Newton parameters");
+    if (params->injection == 1 && (params->well_cell < 0 || params->well_cell >= nf))
+        return fail(EQD_ERR_ARG, "well_cell out of range");
+    const int nnz = ap_ptr[nf];
+    for (int i = 0; i < nf; ++i)
+        if (ap_ptr[i + 1] < ap_ptr[i]) return fail(EQD_ERR_ARG, "Ap row pointers must be non-decreasing");
+    for (int k = 0; k < nnz; ++k)
+        if (ap_idx[k] < 0 || ap_idx[k] >= nf) return fail(EQD_ERR_ARG, "Ap column index out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev) return fail(EQD_ERR_ARG, "device ordinal out of range");
+    CUDA_OR_RETURN(cudaSetDevice(device));
+    std::unique_ptr<eqd_rhs> R(new eqd_rhs());
+    R->device = device;
+    R->nf = nf;
+    R->p = *params;
+    const long long n = 2LL * nf;
+    R->nslice = gemv_slices((int)n);
+    CUDA_OR_RETURN(cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking));
+    CUDA_OR_RETURN(R->K.ensure(sizeof(double) * n * n));
+    CUDA_OR_RETURN(R->part.ensure(sizeof(double) * n * R->nslice));
+    CUDA_OR_RETURN(R->u.ensure(sizeof(double) * (4LL * nf + 1)));
+    CUDA_OR_RETURN(R->du.ensure(sizeof(double) * (4LL * nf + 1)));
+    CUDA_OR_RETURN(R->ap_ptr.ensure(sizeof(int) * (nf + 1)));
+    CUDA_OR_RETURN(R->ap_idx.ensure(sizeof(int) * std::max(nnz, 1)));
+    CUDA_OR_RETURN(R->ap_val.ensure(sizeof(double) * std::max(nnz, 1)));
+    CUDA_OR_RETURN(R->source.ensure(sizeof(double) * nf));
+    CUDA_OR_RETURN(R->active.ensure(nf));
+    CUDA_OR_RETURN(R->vprev.ensure(sizeof(double) * nf));
+    CUDA_OR_RETURN(R->tau.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(R->sigma_low.ensure(sizeof(double) * nf));
+    CUDA_OR_RETURN(R->floor_nodes.ensure(nf));
+    CUDA_OR_RETURN(R->floor_hits.ensure(sizeof(unsigned long long)));
+    CUDA_OR_RETURN(R->status.ensure(sizeof(unsigned)));
+    cudaStream_t st = R->stream;
+    CUDA_OR_RETURN(cudaMemcpyAsync(R->K.p, K, sizeof(double) * n * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_RETURN(cudaMemcpyAsync(R->ap_ptr.p, ap_ptr, sizeof(int) * (nf + 1), cudaMemcpyHostToDevice, st));
+    if (nnz > 0) {
+        CUDA_OR_RETURN(cudaMemcpyAsync(R->ap_idx.p, ap_idx, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+        CUDA_OR_RETURN(cudaMemcpyAsync(R->ap_val.p, ap_val, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+    }
+    if (source) CUDA_OR_RETURN(cudaMemcpyAsync(R->source.p, source, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    else CUDA_OR_RETURN(cudaMemsetAsync(R->source.p, 0, sizeof(double) * nf, st));
+    if (active) CUDA_OR_RETURN(cudaMemcpyAsync(R->active.p, active, nf, cudaMemcpyHostToDevice, st));
+    else CUDA_OR_RETURN(cudaMemsetAsync(R->active.p, 1, nf, st));
+    std::vector<double> init(nf, 1e-12), low(nf, INFINITY);
+    CUDA_OR_RETURN(cudaMemcpyAsync(R->vprev.p, init.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    CUDA_OR_RETURN(cudaMemcpyAsync(R->sigma_low.p, low.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    CUDA_OR_RETURN(cudaMemsetAsync(R->floor_nodes.p, 0, nf, st));
+    CUDA_OR_RETURN(cudaMemsetAsync(R->floor_hits.p, 0, sizeof(unsigned long long), st));
+    CUDA_OR_RETURN(cudaMemsetAsync(R->tau.p, 0, sizeof(double) * n, st));
+    CUDA_OR_RETURN(cudaStreamSynchronize(st));
+    *out = R.release();
+    return EQD_OK;
+}
+
+extern "C" int eqd_rhs_eval(eqd_rhs *R, double t, const double *u, double *du) {
+    if (!R || !u || !du) return fail(EQD_ERR_ARG, "invalid argument");
+    CUDA_OR_RETURN(cudaSetDevice(R->device));
+    const int nf = R->nf;
+    const long long nu = 4LL * nf + (R->p.injection == 1 ? 1 : 0);
+    const long long n = 2LL * nf;
+    cudaStream_t st = R->stream;
+    CUDA_OR_RETURN(cudaMemcpyAsync(R->u.p, u, sizeof(double) * nu, cudaMemcpyHostToDevice, st));
+    CUDA_OR_RETURN(cudaMemsetAsync(R->status.p, 0, sizeof(unsigned), st));
+    dim3 g1((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)R->nslice);
+    gemv_partial_kernel<<<g1, 256, 0, st>>>(R->K.as<double>(), R->u.as<double>(), n, R->nslice, 1,
+                                            R->part.as<double>());
+    RhsParams P{};
+    P.fr = friction_const(R->p);
+    P.sigma0 = R->p.sigma0;
+    P.sigma_min = R->p.sigma_min;
+    P.eta = R->p.eta;
+    P.tau0_2 = R->p.tau0_2;
+    P.tau0_3 = R->p.tau0_3;
+    P.src_scale = t < R->p.t_off ? R->p.q0 / (R->p.beta * R->p.phi) : 0.0;
+    P.tol = R->p.newton_tol;
+    P.maxstep = R->p.newton_maxstep;
+    P.maxiter = R->p.newton_maxiter;
+    P.nf = nf;
+    P.nslice = R->nslice;
+    P.peaceman = R->p.injection == 1;
+    P.well_cell = R->p.well_cell;
+    P.WI = R->p.WI;
+    P.S_e = R->p.S_e;
+    P.S_well = R->p.S_well;
+    P.Qinj = t < R->p.t_off ? R->p.Q0 : 0.0;
+    rhs_node_kernel<<<(unsigned)((nf + 127) / 128), 128, 0, st>>>(
+        P, R->part.as<double>(), R->u.as<double>(), R->du.as<double>(), R->ap_ptr.as<int>(), R->ap_idx.as<int>(),
+        R->ap_val.as<double>(), R->source.as<double>(), R->active.as<unsigned char>(), R->vprev.as<double>(),
+        R->tau.as<double>(), R->sigma_low.as<double>(), R->floor_nodes.as<unsigned char>(),
+        R->floor_hits.as<unsigned long long>(), R->status.as<unsigned>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    unsigned h = 0;
+    CUDA_OR_RETURN(cudaMemcpyAsync(du, R->du.p, sizeof(double) * nu, cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaMemcpyAsync(&h, R->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaStreamSynchronize(st));
+    if (h & RHS_NEWTON_FAILED)
+        return fail(EQD_ERR_NOT_CONVERGED, "solve_slip_rate did not converge at some fault node");
+    return EQD_OK;
+}
+
+extern "C" int eqd_rhs_fields(eqd_rhs *R, double *tau, double *vprev) {
+    if (!R) return fail(EQD_ERR_ARG, "invalid argument");
+    CUDA_OR_RETURN(cudaSetDevice(R->device));
+    if (tau)
+        CUDA_OR_RETURN(cudaMemcpyAsync(tau, R->tau.p, sizeof(double) * 2 * R->nf, cudaMemcpyDeviceToHost, R->stream));
+    if (vprev)
+        CUDA_OR_RETURN(cudaMemcpyAsync(vprev, R->vprev.p, sizeof(double) * R->nf, cudaMemcpyDeviceToHost, R->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(R->stream));
+    return EQD_OK;
+}
+
+extern "C" int eqd_rhs_report(eqd_rhs *R, double *sigma_lowest, int64_t *floor_hits, int32_t *floor_nodes) {
+    if (!R) return fail(EQD_ERR_ARG, "invalid argument");
+    CUDA_OR_RETURN(cudaSetDevice(R->device));
+    std::vector<double> low(R->nf);
+    std::vector<unsigned char> fn(R->nf);
+    unsigned long long hits = 0;
+    CUDA_OR_RETURN(cudaMemcpyAsync(low.data(), R->sigma_low.p, sizeof(double) * R->nf, cudaMemcpyDeviceToHost, R->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(fn.data(), R->floor_nodes.p, R->nf, cudaMemcpyDeviceToHost, R->stream));
+    CUDA_OR_RETURN(cudaMemcpyAsync(&hits, R->floor_hits.p, sizeof(hits), cudaMemcpyDeviceToHost, R->stream));
+    CUDA_OR_RETURN(cudaStreamSynchronize(R->stream));
+    double m = INFINITY;
+    int cnt = 0;
+    for (int i = 0; i < R->nf; ++i) {
+        m = std::min(m, low[i]);
+        cnt += fn[i] != 0;
+    }
+    if (sigma_lowest) *sigma_lowest = m;
+    if (floor_hits) *floor_hits = (int64_t)hits;
+    if (floor_nodes) *floor_nodes = cnt;
+    return EQD_OK;
+}
+
+extern "C" int eqd_rhs_destroy(eqd_rhs *R) {
+    if (!R) return EQD_OK;
+    cudaSetDevice(R->device);
+    if (R->stream) {
+        cudaStreamSynchronize(R->stream);
+        cudaStreamDestroy(R->stream);
+    }
+    delete R;
+    return EQD_OK;
+}
+
+extern "C" int eqd_friction_solve(int32_t device, int32_t n, const double *T, const double *theta, const double *sigma,
+                                  double eta, const eqd_rhs_params *params, const double *V0, double *V) {
+    if (n < 0 || (n > 0 && (!T || !theta || !sigma || !V)) || !params) return fail(EQD_ERR_ARG, "invalid argument");
+    if (!newton_ok(*params)) return fail(EQD_ERR_ARG, "invalid friction or Newton parameters");
+    if (n == 0) return EQD_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(EQD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev) return fail(EQD_ERR_ARG, "device ordinal out of range");
+    CUDA_OR_RETURN(cudaSetDevice(device));
+    DevBuf dT, dth, dsg, dv0, dV, dst;
+    CUDA_OR_RETURN(dT.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(dth.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(dsg.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(dV.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(dst.ensure(sizeof(unsigned)));
+    if (V0) CUDA_OR_RETURN(dv0.ensure(sizeof(double) * n));
+    CUDA_OR_RETURN(cudaMemcpy(dT.p, T, sizeof(double) * n, cudaMemcpyHostToDevice));
+    CUDA_OR_RETURN(cudaMemcpy(dth.p, theta, sizeof(double) * n, cudaMemcpyHostToDevice));
+    CUDA_OR_RETURN(cudaMemcpy(dsg.p, sigma, sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (V0) CUDA_OR_RETURN(cudaMemcpy(dv0.p, V0, sizeof(double) * n, cudaMemcpyHostToDevice));
+    CUDA_OR_RETURN(cudaMemset(dst.p, 0, sizeof(unsigned)));
+    friction_solve_kernel<<<(unsigned)((n + 127) / 128), 128>>>(
+        n, dT.as<double>(), dth.as<double>(), dsg.as<double>(), eta, friction_const(*params),
+        V0 ? dv0.as<double>() : nullptr, params->newton_tol, params->newton_maxiter, params->newton_maxstep,
+        dV.as<double>(), dst.as<unsigned>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    unsigned h = 0;
+    CUDA_OR_RETURN(cudaMemcpy(V, dV.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CUDA_OR_RETURN(cudaMemcpy(&h, dst.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (h & RHS_NEWTON_FAILED)
+        return fail(EQD_ERR_NOT_CONVERGED, "solve_slip_rate failed to converge");
     return EQD_OK;
 }

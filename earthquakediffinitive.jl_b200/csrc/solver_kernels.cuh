@@ -519,38 +519,71 @@ __global__ void toeplitz_expand_kernel(const double *__restrict__ src_cols, cons
 
 // ---------------------------------------------------------------------------
 // Dense FP64 GEMV y = K s (K column-major n x n), two passes: column slices
-// write partial row sums, then a fixed-order reduction over slices.
+// write partial row sums, then a fixed-order reduction over slices. Vectors
+// go four at a time, so one pass over K serves four right-hand sides (the
+// time loop's Runge-Kutta stages or an ensemble): K is read ceil(nvec / 4)
+// times instead of nvec times.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restrict__ K, const double *__restrict__ s,
                                                            long long n, int nslice, int nvec,
                                                            double *__restrict__ part) {
+    constexpr int VB = 4;
     const long long row2 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
     const int slice = blockIdx.y;
     const long long c0 = n * slice / nslice, c1 = n * (slice + 1) / nslice;
-    for (int v = 0; v < nvec; ++v) {
-        const double *sv = s + (long long)v * n;
-        double a0 = 0.0, a1 = 0.0;
+    for (int v0 = 0; v0 < nvec; v0 += VB) {
+        const int nv = min(VB, nvec - v0);
+        const double *sv[VB];
+#pragma unroll
+        for (int u = 0; u < VB; ++u) sv[u] = s + (long long)(v0 + (u < nv ? u : 0)) * n;
+        double a0[VB], a1[VB];
+#pragma unroll
+        for (int u = 0; u < VB; ++u) a0[u] = a1[u] = 0.0;
         if (row2 + 1 < n) {
             long long c = c0;
-            for (; c + 4 <= c1; c += 4) {
-                const double2 k0 = *reinterpret_cast<const double2 *>(K + c * n + row2);
-                const double2 k1 = *reinterpret_cast<const double2 *>(K + (c + 1) * n + row2);
-                const double2 k2 = *reinterpret_cast<const double2 *>(K + (c + 2) * n + row2);
-                const double2 k3 = *reinterpret_cast<const double2 *>(K + (c + 3) * n + row2);
-                const double s0 = sv[c], s1 = sv[c + 1], s2 = sv[c + 2], s3 = sv[c + 3];
-                a0 += k0.x * s0 + k1.x * s1 + k2.x * s2 + k3.x * s3;
-                a1 += k0.y * s0 + k1.y * s1 + k2.y * s2 + k3.y * s3;
+            for (; c + 4 <= c1; c += 4) {  // four columns in flight per thread
+                double2 kk[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) kk[j] = *reinterpret_cast<const double2 *>(K + (c + j) * n + row2);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                    for (int u = 0; u < VB; ++u) {
+                        if (u < nv) {
+                            const double sc = sv[u][c + j];
+                            a0[u] += kk[j].x * sc;
+                            a1[u] += kk[j].y * sc;
+                        }
+                    }
+                }
             }
             for (; c < c1; ++c) {
                 const double2 kk = *reinterpret_cast<const double2 *>(K + c * n + row2);
-                a0 += kk.x * sv[c];
-                a1 += kk.y * sv[c];
+#pragma unroll
+                for (int u = 0; u < VB; ++u) {
+                    if (u < nv) {
+                        const double sc = sv[u][c];
+                        a0[u] += kk.x * sc;
+                        a1[u] += kk.y * sc;
+                    }
+                }
             }
-            part[((long long)v * nslice + slice) * n + row2] = a0;
-            part[((long long)v * nslice + slice) * n + row2 + 1] = a1;
+#pragma unroll
+            for (int u = 0; u < VB; ++u) {
+                if (u < nv) {
+                    part[((long long)(v0 + u) * nslice + slice) * n + row2] = a0[u];
+                    part[((long long)(v0 + u) * nslice + slice) * n + row2 + 1] = a1[u];
+                }
+            }
         } else if (row2 < n) {
-            for (long long c = c0; c < c1; ++c) a0 += K[c * n + row2] * sv[c];
-            part[((long long)v * nslice + slice) * n + row2] = a0;
+            for (long long c = c0; c < c1; ++c) {
+                const double kk = K[c * n + row2];
+#pragma unroll
+                for (int u = 0; u < VB; ++u) a0[u] += kk * sv[u][c];
+            }
+#pragma unroll
+            for (int u = 0; u < VB; ++u)
+                if (u < nv) part[((long long)(v0 + u) * nslice + slice) * n + row2] = a0[u];
         }
     }
 }

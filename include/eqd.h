@@ -210,6 +210,57 @@ int eqd_kmat_destroy(eqd_kmat *kmat);
 int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_device, const double *s_device,
                          double *y_device, int32_t nvec, void *stream);
 
+/* Time-loop right-hand side of the coupled BP8 model -----------------------
+ * `rhs!(du, u, m, t)` / `evaluate!(m, u, t)` (src/BP8.jl:356-433) with K
+ * resident on the GPU: Δτ = K·[s2; s3] (the GEMV), the slip velocity from
+ * the radiation-damped rate-and-state force balance per fault node
+ * (`solve_slip_velocity`, src/RateStateFriction.jl:77-117: Newton in ln V,
+ * steps clamped to newton_maxstep, warm-started from the previous slip
+ * rate), the aging law in φ = ln θ, and the pore-pressure equation
+ * dp/dt = Ap·p + injection with the caller's sparse Ap (CSR, 0-based).
+ * State u = [s2; s3; φ; p] (4nf), plus the well pressure for the Peaceman
+ * well (4nf + 1); du has the same layout. */
+typedef struct {
+    double a, b, Dc, V_star, f_star;   /* FrictionParams (Dc = D_RS) */
+    double sigma0, sigma_min;          /* effective normal stress and its floor (Pa) */
+    double eta;                        /* radiation damping mu / (2 c_s) */
+    double tau0_2, tau0_3;             /* background shear traction (Pa) */
+    double q0, beta, phi, t_off;       /* Gaussian source: q0 / (beta phi) * source while t < t_off */
+    int32_t injection;                 /* 0 Gaussian source, 1 Peaceman well */
+    int32_t well_cell;                 /* 0-based node of the well */
+    double WI, S_e, S_well, Q0;        /* Peaceman well */
+    double newton_tol;                 /* 1e-12 */
+    double newton_maxstep;             /* 5.0 */
+    int32_t newton_maxiter;            /* 50 */
+    int32_t pad_;
+} eqd_rhs_params;
+
+typedef struct eqd_rhs eqd_rhs;
+
+/* K: 2nf x 2nf column-major (host); Ap: nf x nf CSR (ap_ptr[nf+1], ap_idx,
+ * ap_val); source (nf, Gaussian injection) and active (nf, 0 = locked node)
+ * may be NULL (zeros / all active). */
+int eqd_rhs_create(int32_t device, int32_t nf, const double *K, const eqd_rhs_params *params, const int32_t *ap_ptr,
+                   const int32_t *ap_idx, const double *ap_val, const double *source, const uint8_t *active,
+                   eqd_rhs **out);
+/* du = rhs(u, t) (host arrays). EQD_ERR_NOT_CONVERGED if a Newton solve did
+ * not converge (the reference throws). */
+int eqd_rhs_eval(eqd_rhs *rhs, double t, const double *u, double *du);
+/* The cache fields of the last evaluation: shear stress acting on the fault
+ * tau (2nf: τ2 then τ3) and the warm-start slip rate Vprev (nf); either may
+ * be NULL. */
+int eqd_rhs_fields(eqd_rhs *rhs, double *tau, double *vprev);
+/* `effective_stress_report` inputs: lowest σ̄ = σ0 - p seen before the floor,
+ * how many node evaluations hit the floor, and how many nodes ever did. */
+int eqd_rhs_report(eqd_rhs *rhs, double *sigma_lowest, int64_t *floor_hits, int32_t *floor_nodes);
+int eqd_rhs_destroy(eqd_rhs *rhs);
+
+/* `solve_slip_rate` for n independent nodes (src/RateStateFriction.jl:77-100):
+ * V[i] solves T = eta V + sigma a asinh(V/(2V*) C(theta)), seeded from V0[i]
+ * (NULL: V*). Uses the friction and Newton fields of `params`. */
+int eqd_friction_solve(int32_t device, int32_t n, const double *T, const double *theta, const double *sigma,
+                       double eta, const eqd_rhs_params *params, const double *V0, double *V);
+
 /* Serving: stiffness-column requests answered by continuous batching -------
  * The reference builds K in one blocking call (`fault_stiffness`,
  * src/FaultResponse.jl:229-287, its column loop `run_columns!` :244-263).

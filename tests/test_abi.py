@@ -65,6 +65,8 @@ def test_struct_layouts(built):
     assert C.sizeof(eqd._abi.SolveOpts) == 64
     assert C.sizeof(eqd._abi.Stats) == 72
     assert C.sizeof(eqd._abi.RequestInfo) == 48
+    from eqd_b200.timeloop import RhsParams
+    assert C.sizeof(RhsParams) == 176
 
 
 def test_defaults_match_reference_cgsolver(built):

@@ -158,9 +158,10 @@ def test_gemv(eqd):
     s = rng.standard_normal(n)
     y = M.gemv(s)
     assert np.allclose(y, K @ s, rtol=1e-12, atol=1e-12 * abs(K).sum(1).max())
-    S = rng.standard_normal((n, 3))
-    Y = M.gemv(S)
-    assert np.allclose(Y, K @ S, rtol=1e-12, atol=1e-10)
+    for nv in (3, 4, 9):  # vector groups of four, with remainders
+        S = rng.standard_normal((n, nv))
+        Y = M.gemv(S)
+        assert np.allclose(Y, K @ S, rtol=1e-12, atol=1e-10)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -215,3 +216,16 @@ def test_mixed_corner_columns_bp8_scale(eqd):
     K64 = eqd.stiffness_columns(fe64, cols)[0]
     assert (st == 1).all(), (st, it)
     assert rel(K, K64) < K_TOL
+
+
+def test_cached_fault_stiffness(eqd, tmp_path):
+    """The on-disk K cache built by the GPU in column blocks equals the
+    one-call build bit for bit, and a second call loads it."""
+    fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4)
+    eqd.set_stencil_variant(fe, 1)
+    K = eqd.fault_stiffness(fe)
+    Kc = eqd.cached_fault_stiffness(fe, str(tmp_path), block=16)
+    assert np.array_equal(Kc, K)
+    solves = eqd.solver_report(fe.rs)["solves"]
+    Kc2 = eqd.cached_fault_stiffness(fe, str(tmp_path), block=16)
+    assert np.array_equal(Kc2, K) and eqd.solver_report(fe.rs)["solves"] == solves
