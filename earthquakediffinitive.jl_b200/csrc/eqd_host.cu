@@ -161,6 +161,34 @@ static void fill_op(OpConst<T> &C, const GridConst &gc, const double h[3]) {
     C.hvol = gc.hvol;
 }
 
+// Page-locked host array: device-to-host copies into it stay asynchronous.
+template <typename E>
+struct PinnedArr {
+    E *p = nullptr;
+    int n = 0;
+    PinnedArr() = default;
+    PinnedArr(const PinnedArr &) = delete;
+    PinnedArr &operator=(const PinnedArr &) = delete;
+    ~PinnedArr() {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t assign(int count, E v) {
+        if (count > n) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            n = 0;
+            cudaError_t e = cudaHostAlloc((void **)&p, sizeof(E) * std::max(count, 1), cudaHostAllocDefault);
+            if (e != cudaSuccess) return e;
+            n = count;
+        }
+        for (int i = 0; i < count; ++i) p[i] = v;
+        return cudaSuccess;
+    }
+    E *data() { return p; }
+    E &operator[](int i) { return p[i]; }
+    const E &operator[](int i) const { return p[i]; }
+};
+
 // Workspace of one batched solve (grown on demand, reused across calls).
 struct Workspace {
     int cap = 0;            // columns
@@ -172,6 +200,7 @@ struct Workspace {
     DevBuf kout;
     DevBuf newmask, slot_list, dst_list;  // slot engine: entering columns, extraction lists
     DevBuf hbuf;                          // explicit-RHS staging (reference layout)
+    PinnedArr<double> kstage;             // finished K columns on their way to a host K
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     std::vector<double> graph_key;  // what the captured graph baked in (see SlotRun::setup)
@@ -821,34 +850,6 @@ struct ColDone {
 
 static int tune_by_iterations(eqd_grid *G, const eqd_solve_opts &o, int ncols);
 
-// Page-locked host array: device-to-host copies into it stay asynchronous.
-template <typename E>
-struct PinnedArr {
-    E *p = nullptr;
-    int n = 0;
-    PinnedArr() = default;
-    PinnedArr(const PinnedArr &) = delete;
-    PinnedArr &operator=(const PinnedArr &) = delete;
-    ~PinnedArr() {
-        if (p) cudaFreeHost(p);
-    }
-    cudaError_t assign(int count, E v) {
-        if (count > n) {
-            if (p) cudaFreeHost(p);
-            p = nullptr;
-            n = 0;
-            cudaError_t e = cudaHostAlloc((void **)&p, sizeof(E) * std::max(count, 1), cudaHostAllocDefault);
-            if (e != cudaSuccess) return e;
-            n = count;
-        }
-        for (int i = 0; i < count; ++i) p[i] = v;
-        return cudaSuccess;
-    }
-    E *data() { return p; }
-    E &operator[](int i) { return p[i]; }
-    const E &operator[](int i) const { return p[i]; }
-};
-
 template <typename T>
 struct SlotRun {
     eqd_grid *G = nullptr;
@@ -1232,8 +1233,9 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
         c.rhs = B.rhs ? B.rhs + (size_t)i * ntot : nullptr;
     }
     int64_t tot_it = 0, max_it = 0, unconv = 0;
-    std::vector<double> kstage;
-    if (!generic && B.kcols && !B.kdev) kstage.resize((size_t)2 * gc.nf * chunk);
+    PinnedArr<double> &kstage = R.W->kstage;
+    if (!generic && B.kcols && !B.kdev && kstage.n < 2 * gc.nf * chunk)
+        CUDA_OR_RETURN(kstage.assign(2 * gc.nf * chunk, 0.0));
     CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
     int next = 0, finished = 0;
     std::vector<ColDone> done;

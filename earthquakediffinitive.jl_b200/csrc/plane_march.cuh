@@ -330,6 +330,14 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const int nI = ihi - ilo;
     const int per = 2 * (n1 - 1);
     const int C0 = nI * per, C1 = (T2 - nI) * per, C2 = 2 * T2;  // threads per class
+    // Each class starts on a warp boundary when the CTA has the threads for
+    // it: a warp that mixed classes would pay for both classes' extra work
+    // (x2 closure corrections and the fault-face SAT path), and the
+    // per-plane barrier waits for the slowest warp.
+    const int P0 = (C0 + 31) & ~31, P1 = (C1 + 31) & ~31;
+    const bool aligned = P0 + P1 + C2 <= (int)blockDim.x;
+    const int B0 = aligned ? P0 : C0;           // first thread of class 1
+    const int B1 = B0 + (aligned ? P1 : C1);    // first thread of class 2 (even)
     int side = 0, i2 = a0, i1 = 0, cls = 3;
     if (tid < C0) {
         const int rr = tid / per, q = tid % per;
@@ -338,8 +346,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         i1 = side == 0 ? j : j + 1;
         i2 = ilo + rr;
         cls = 0;
-    } else if (tid < C0 + C1) {
-        const int k = tid - C0;
+    } else if (tid >= B0 && tid < B0 + C1) {
+        const int k = tid - B0;
         const int rr = k / per, q = k % per;
         side = q / (n1 - 1);
         const int j = q % (n1 - 1);
@@ -347,8 +355,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         const int nlow = ilo - a0;
         i2 = rr < nlow ? a0 + rr : ihi + (rr - nlow);
         cls = 1;
-    } else if (tid < C0 + C1 + C2) {
-        const int k = tid - C0 - C1;
+    } else if (tid >= B1 && tid < B1 + C2) {
+        const int k = tid - B1;
         side = k & 1;
         i1 = side == 0 ? n1 - 1 : 0;
         i2 = a0 + (k >> 1);

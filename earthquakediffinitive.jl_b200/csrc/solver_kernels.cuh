@@ -381,16 +381,6 @@ __global__ void jacobi_diag_kernel(const __grid_constant__ OpConst<double> C, in
     if (dinv32) dinv32[idx] = (float)inv;
 }
 
-__global__ void count_active_kernel(const int8_t *__restrict__ status, int ncols, int *__restrict__ out) {
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    int c = 0;
-    for (int i = threadIdx.x; i < ncols; i += blockDim.x) c += status[i] == COL_ACTIVE;
-    atomicAdd(&cnt, c);
-    __syncthreads();
-    if (threadIdx.x == 0) *out = cnt;
-}
 
 // ---------------------------------------------------------------------------
 // Traction extraction: K column entries from U = x + chi (FP64).
