@@ -65,9 +65,12 @@ class Server:
     `hbm_budget_bytes` (0: free device memory minus 2 GiB)."""
 
     def __init__(self, hbm_budget_bytes=0, rtol=1e-10, atol=0.0, itmax=0, precision="mixed", reliable_delta=0.01,
-                 split=True):
+                 split=True, precond="none"):
         o = _abi.default_opts()
         o.rtol, o.atol, o.itmax = float(rtol), float(atol), int(itmax)
+        if precond not in ("none", "jacobi"):
+            raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precond must be :none or :jacobi, got {precond}")
+        o.precond = _abi.EQD_PRECOND_JACOBI if precond == "jacobi" else _abi.EQD_PRECOND_NONE
         if precision not in ("mixed", "fp64"):
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precision must be 'mixed' or 'fp64', got {precision}")
         o.precision = _abi.EQD_PREC_MIXED if precision == "mixed" else _abi.EQD_PREC_FP64

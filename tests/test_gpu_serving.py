@@ -66,6 +66,20 @@ def test_server_owns_its_grids_and_validates(eqd):
 
 def test_budget_limits_slots(eqd):
     sa, _ = _grids(eqd, "mixed")
-    with eqd.Server(hbm_budget_bytes=1 << 20) as srv:   # 1 MiB: not even one slot of 11^3 x 6 DOF
+    with eqd.Server(hbm_budget_bytes=1 << 20) as srv:   # 1 MiB: room for a few slots of this grid, not 64
         with pytest.raises(eqd.EqdError):
             srv.add(sa, slots=64)
+
+
+def test_server_with_jacobi(eqd):
+    """Jacobi-preconditioned serving gives the same bits as a Jacobi batch."""
+    ra = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4, precond="jacobi")
+    sa = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4)
+    for fe in (ra, sa):
+        eqd.set_stencil_variant(fe, 1)
+    cols = np.array([0, 7, 31, 49])
+    with eqd.Server(hbm_budget_bytes=1 << 30, precond="jacobi") as srv:
+        srv.add(sa, slots=3)
+        K = srv.submit(sa, cols).result(timeout=120)
+    K_ref, it_ref, _ = eqd.stiffness_columns(ra, cols)
+    assert np.array_equal(K, K_ref)
