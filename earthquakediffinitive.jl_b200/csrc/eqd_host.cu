@@ -203,7 +203,7 @@ struct Workspace {
     PinnedArr<double> kstage;             // finished K columns on their way to a host K
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
-    std::vector<double> graph_key;  // what the captured graph baked in (see SlotRun::setup)
+    std::vector<uint64_t> graph_key;  // what the captured graph baked in (see SlotRun::setup)
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
     }
@@ -945,18 +945,17 @@ struct SlotRun {
         // Everything the captured kernels bake in: sizes, options and every
         // workspace pointer (a buffer that grew or was released since the
         // capture must not be reached through the old graph).
-        const double key[] = {(double)cap, (double)o.precision, (double)generic, (double)G->sel32,
-                              (double)o.precond, (double)split, sp.rtol, sp.atol, (double)sp.itmax, sp.delta,
-                              (double)(uintptr_t)w.x64.p, (double)(uintptr_t)w.v0.p, (double)(uintptr_t)w.v1.p,
-                              (double)(uintptr_t)w.v2.p, (double)(uintptr_t)w.v3.p, (double)(uintptr_t)w.apply_part.p,
-                              (double)(uintptr_t)w.res_part.p, (double)(uintptr_t)w.rr_part.p,
-                              (double)(uintptr_t)w.gamma.p, (double)(uintptr_t)w.beta.p, (double)(uintptr_t)w.rr_ref.p,
-                              (double)(uintptr_t)w.tol.p, (double)(uintptr_t)w.bnorm.p, (double)(uintptr_t)w.iters.p,
-                              (double)(uintptr_t)w.status.p, (double)(uintptr_t)w.flag.p,
-                              (double)(uintptr_t)w.slip_node.p, (double)(uintptr_t)w.slip_comp.p,
-                              (double)(uintptr_t)w.slip_dense.p, (double)(uintptr_t)G->dinv64.p,
-                              (double)(uintptr_t)G->dinv32.p};
-        const std::vector<double> kv(std::begin(key), std::end(key));
+        std::vector<uint64_t> kv = {(uint64_t)cap, (uint64_t)o.precision, (uint64_t)generic, (uint64_t)G->sel32,
+                                    (uint64_t)o.precond, (uint64_t)split, (uint64_t)sp.itmax};
+        for (double d : {sp.rtol, sp.atol, sp.delta}) {
+            uint64_t b;
+            std::memcpy(&b, &d, sizeof(b));
+            kv.push_back(b);
+        }
+        for (const void *q : {w.x64.p, w.v0.p, w.v1.p, w.v2.p, w.v3.p, w.apply_part.p, w.res_part.p, w.rr_part.p,
+                              w.gamma.p, w.beta.p, w.rr_ref.p, w.tol.p, w.bnorm.p, w.iters.p, w.status.p, w.flag.p,
+                              w.slip_node.p, w.slip_comp.p, w.slip_dense.p, G->dinv64.p, G->dinv32.p})
+            kv.push_back((uint64_t)(uintptr_t)q);
         if (!w.graph || w.graph_key != kv) {
             if (w.graph) cudaGraphExecDestroy(w.graph);
             w.graph = nullptr;
