@@ -10,9 +10,11 @@ the reference package.
 """
 module EqdB200
 
+using LinearAlgebra
+
 export GpuFaultElasticity, gpu_fault_stiffness, gpu_fault_stiffness_toeplitz,
        gpu_shear_traction, GpuK, gpu_mul!, gpu_solver_report,
-       GpuServer, serve!, submit, wait_request, request_info
+       GpuServer, serve!, submit, wait_request, request_info, GpuSplitNodeOperator
 
 const libeqd = get(ENV, "EQD_LIB", joinpath(@__DIR__, "..", "lib", "libeqd.so"))
 
@@ -132,6 +134,43 @@ gpu_solver_report(fe::GpuFaultElasticity) =
        iterations=fe.stats.iterations,
        mean_iterations=fe.stats.solves == 0 ? 0.0 : fe.stats.iterations / fe.stats.solves,
        max_iterations=fe.stats.max_iterations, unconverged=fe.stats.unconverged)
+
+"""
+    GpuSplitNodeOperator(fe; mode=:A, precision=:fp64)
+
+The split-node operator as a matrix-free linear map on the GPU, for callers
+that want `A` or `HP_DSAT` (src/ElasticitySplitNode.jl:210-211) without
+assembling them: `mul!(y, op, x)` applies `A = -HP(D+SAT)P` (`mode=:A`) or
+`HP(D+SAT)` (`mode=:HP_DSAT`) to vectors in the reference DOF layout, so
+Krylov.jl on the host can drive the GPU stencil.
+"""
+struct GpuSplitNodeOperator
+    fe::GpuFaultElasticity
+    mode::Int32
+    precision::Int32
+    n::Int
+end
+
+function GpuSplitNodeOperator(fe::GpuFaultElasticity; mode=:A, precision=:fp64)
+    ntot = Ref{Int64}(0); nf = Ref{Int32}(0); n2f = Ref{Int32}(0); n3f = Ref{Int32}(0)
+    check(ccall((:eqd_grid_info, libeqd), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int32}, Ref{Int32}, Ref{Int32}),
+                fe.handle, ntot, nf, n2f, n3f))
+    mode in (:A, :HP_DSAT) || error("mode must be :A or :HP_DSAT, got $mode")
+    return GpuSplitNodeOperator(fe, mode === :A ? 0 : 1, precision === :fp64 ? 0 : 1, Int(ntot[]))
+end
+
+Base.size(op::GpuSplitNodeOperator) = (op.n, op.n)
+Base.size(op::GpuSplitNodeOperator, d::Integer) = d <= 2 ? op.n : 1
+Base.eltype(::GpuSplitNodeOperator) = Float64
+
+function LinearAlgebra.mul!(y::AbstractVecOrMat{Float64}, op::GpuSplitNodeOperator, x::AbstractVecOrMat{Float64})
+    size(x, 1) == op.n && size(y) == size(x) || throw(DimensionMismatch("operator is $(op.n) x $(op.n)"))
+    xc = Matrix{Float64}(reshape(x, op.n, :)); yc = similar(xc)
+    check(ccall((:eqd_apply, libeqd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32, Int32, Int32),
+                op.fe.handle, xc, yc, size(xc, 2), op.mode, op.precision))
+    copyto!(y, yc)
+    return y
+end
 
 "K resident on the device for the time loop's `mul!(Δτ, K, slip)` (src/BP8.jl:366)."
 mutable struct GpuK
