@@ -301,9 +301,9 @@ def main():
     # Autotuner evidence: every FP32 launch variant timed on the batch.
     sel = C.c_int32()
     nv = C.c_int32()
-    tms = (C.c_double * 8)()
-    trows = (C.c_int32 * 8)()
-    tthr = (C.c_int32 * 8)()
+    tms = (C.c_double * 16)()
+    trows = (C.c_int32 * 16)()
+    tthr = (C.c_int32 * 16)()
     eqd._abi.check(lib.eqd_autotune(fe.handle, C.c_int32(min(len(cols), 512)), C.byref(sel), tms, trows, tthr,
                                     C.byref(nv)))
     autotune = {"selected": sel.value,

@@ -248,7 +248,7 @@ def set_stencil_variant(fe, variant):
 def autotune(fe, ncols=256):
     """Time every FP32 stencil launch variant; returns (selected, [(tile_rows, threads, ms)])."""
     sel, nv = C.c_int32(), C.c_int32()
-    ms, tr, tt = (C.c_double * 8)(), (C.c_int32 * 8)(), (C.c_int32 * 8)()
+    ms, tr, tt = (C.c_double * 16)(), (C.c_int32 * 16)(), (C.c_int32 * 16)()
     check(lib().eqd_autotune(fe.handle, C.c_int32(ncols), C.byref(sel), ms, tr, tt, C.byref(nv)))
     return sel.value, [(tr[i], tt[i], ms[i]) for i in range(nv.value)]
 

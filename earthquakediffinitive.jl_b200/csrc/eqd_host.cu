@@ -77,7 +77,7 @@ static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register s
 static constexpr int kMaxT32c = 384;  // FP32 A-apply, two columns per thread
 static constexpr int kMaxT64 = 384;
 static constexpr int kMaxT64b = 512;  // FP64 instances for wide x1 lines (n1 = 33 needs 7 x 66 threads)
-static constexpr int kNumVariants = 7;
+static constexpr int kNumVariants = 9;
 
 static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
 
@@ -467,11 +467,12 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     {
         // thread limit, kernel launch bound, columns per thread, tile rows
         // (0: as many as fit), edge partition
-        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192, kMaxT32b, kMaxT32b};
-        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c, kMaxT32b, kMaxT32b};
-        const int ln[kNumVariants] = {1, 1, 1, 2, 2, 1, 1};
-        const int rows[kNumVariants] = {0, 0, 0, 0, 0, 7, 10};
-        const bool edg[kNumVariants] = {false, false, false, false, false, true, true};
+        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192, kMaxT32b, kMaxT32b, 192, 448};
+        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c, kMaxT32b, kMaxT32b,
+                                      kMaxT32b, kMaxT32b};
+        const int ln[kNumVariants] = {1, 1, 1, 2, 2, 1, 1, 1, 1};
+        const int rows[kNumVariants] = {0, 0, 0, 0, 0, 7, 10, 0, 0};
+        const bool edg[kNumVariants] = {false, false, false, false, false, true, true, false, false};
         for (int v = 0; v < kNumVariants; ++v) {
             G->v32_maxt[v] = mt[v];
             G->v32_lanes[v] = ln[v];

@@ -181,7 +181,7 @@ int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t 
  * size, columns per thread, edge-partitioned tiles): times 20 mixed-precision
  * CG iterations of ncols unit-slip columns (<= 2nf) with every variant, keeps
  * the fastest for this grid (used by every later mixed-precision call) and
- * reports milliseconds per iteration. Arrays hold *nvariants (<= 8) entries. */
+ * reports milliseconds per iteration. Arrays hold *nvariants (<= 16) entries. */
 int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_per_variant, int32_t *tile_rows,
                  int32_t *threads, int32_t *nvariants);
 
