@@ -15,6 +15,7 @@
 #define EQD_MAX_N1 40
 #define EQD_NSLOT 6          // plane ring: p = s-3 .. s in use, two in flight
 #define EQD_HALO 4           // i2 halo rows on each side of a tile (wide D1*D1)
+#define EQD_PBLK 8           // x3 march steps per dot-product partial block
 
 namespace eqd {
 

@@ -142,13 +142,40 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     out.g.i3f0 = gc.i3f0;
     out.g.n3f = gc.n3f;
     out.g.nf = gc.nf;
+    // FP64-input instances sum dot products per x3 step block (and can split
+    // a column along x3); FP32 ones per tile over the whole column.
+    out.g.nblk = sizeof(T) == 8 ? (n3 + EQD_PBLK - 1) / EQD_PBLK : 1;
+    out.g.nseg = 1;
+    out.g.segblk = out.g.nblk;
     int threads = per_row * t2max;
     threads = (threads + 31) / 32 * 32;
     out.threads = threads;
     // barriers + flags, reduction scratch, and per column: plane ring, F1/H21
-    // exchange [2][points] x 2
+    // exchange [2][points] x 2; FP64: per-(step block, warp) dot-product sums
     out.smem = 64 + 32 * 8 + (size_t)lanes * ((size_t)EQD_NSLOT * 6 * CH + 4 * (size_t)NP) * sizeof(T);
+    if (sizeof(T) == 8) out.smem += 16 + (size_t)lanes * out.g.nblk * (threads / 32) * 2 * sizeof(double);
     return true;
+}
+
+// Dot-product partials per column of a launch configuration: one per
+// (x2 tile, x3 step block) for FP64-input configurations, one per x2 tile
+// for FP32 ones (nblk = 1).
+static int nparts(const MarchCfg &m) { return m.g.ntiles * m.g.nblk; }
+
+// x3 segmentation of an FP64-input launch: a batch too small to give every
+// SM two CTAs is split along x3 into segments of whole step blocks (a
+// segment marches 9 to 14 planes before its first block to fill its windows
+// and 3 planes past its last). Partials are per step block, so the results
+// do not depend on the split.
+static MarchCfg segmented(const MarchCfg &m, long long groups, int num_sms) {
+    MarchCfg r = m;
+    const long long ctas = groups * m.g.ntiles;
+    const long long target = 2LL * num_sms;
+    if (ctas >= target || m.g.nblk <= 1) return r;
+    const int want = (int)std::min<long long>((target + ctas - 1) / ctas, m.g.nblk);
+    r.g.segblk = (m.g.nblk + want - 1) / want;
+    r.g.nseg = (m.g.nblk + r.g.segblk - 1) / r.g.segblk;
+    return r;
 }
 
 template <typename T>
@@ -281,9 +308,10 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
     const int n1 = G->gc.n1;
     if (sizeof(T) == 4 && MODE == MODE_A) {
         const int v = variant >= 0 ? variant : G->sel32;
-        const MarchCfg &m = G->v32[v];
         const int lanes = G->v32_lanes[v];
-        dim3 grid((unsigned)(((ncols + lanes - 1) / lanes) * m.g.ntiles));
+        const long long groups = (ncols + lanes - 1) / lanes;
+        const MarchCfg m = segmented(G->v32[v], groups, G->num_sms);
+        dim3 grid((unsigned)(groups * m.g.ntiles * m.g.nseg));
         const float *fin = reinterpret_cast<const float *>(in);
         float *fout = reinterpret_cast<float *>(out);
         if (lanes == 2)
@@ -298,10 +326,10 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
         return cudaGetLastError();
     }
     constexpr int MAXT = sizeof(T) == 4 ? kMaxT32 : kMaxT64;
-    const MarchCfg &m = sizeof(T) == 4 ? G->m32 : G->m64;
+    const MarchCfg m = segmented(sizeof(T) == 4 ? G->m32 : G->m64, ncols, G->num_sms);
     const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
                                                                                : (const void *)&G->c64);
-    dim3 grid((unsigned)(ncols * m.g.ntiles));
+    dim3 grid((unsigned)(ncols * m.g.ntiles * m.g.nseg));
     const bool wide64 = sizeof(T) == 8 && G->m64_maxt == kMaxT64b;
     if (MODE == MODE_AP) {  // generic-input hook: runtime-n1 instance only
         if (wide64)
@@ -584,8 +612,8 @@ static int apply_impl(eqd_grid *G, const double *x, double *y, int ncols, int mo
         CUDA_OR_RETURN((launch_march<T, T, MODE_AP>(G, dx.as<T>(), dy.as<T>(), cs, nullptr, ncols)));
     } else if (mode == 2) {
         DevBuf part;
-        int nt = G->m64.g.ntiles;
-        for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, G->v32[v].g.ntiles);
+        int nt = nparts(G->m64);
+        for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, nparts(G->v32[v]));
         CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * nt));
         CUDA_OR_RETURN((launch_march<T, T, MODE_A>(G, dx.as<T>(), dy.as<T>(), cs, part.as<double>(), ncols)));
     } else {
@@ -687,7 +715,7 @@ static IterPtrs<T> span_ptrs(eqd_grid *G, Workspace &W, const SolveParams &sp, c
     P.d = W.v3.p ? W.v3.as<float>() + c0 * gc.colstride : nullptr;
     P.x64 = W.x64.as<double>() + c0 * gc.colstride;
     P.apply_part = W.apply_part.as<double>() + c0 * sp.ntiles * 2;
-    P.res_part = W.res_part.as<double>() + c0 * G->m64.g.ntiles * 2;
+    P.res_part = W.res_part.as<double>() + c0 * nparts(G->m64) * 2;
     P.rr_part = W.rr_part.as<double>() + c0 * G->nchunks * 2;
     return P;
 }
@@ -746,7 +774,7 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
         cf.dinv = dinv64;
         launch_march<double, float, MODE_RHS>(G, P.x64, (float *)P.r, cf, P.res_part, sn.n, -1, sn.s);
         SolveParams sp2 = sp;
-        sp2.ntiles = G->m64.g.ntiles;
+        sp2.ntiles = nparts(G->m64);
         cg_true_residual_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp2, P.res_part, sn.n, 1);
     }
     const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
@@ -882,15 +910,15 @@ struct SlotRun {
             int rc = tune_by_iterations(G, o, std::min(cap, 1024));
             if (rc) return rc;
         }
-        const int nt32 = G->v32[G->sel32].g.ntiles, nt64 = G->m64.g.ntiles;
+        const int nt32 = nparts(G->v32[G->sel32]), nt64 = nparts(G->m64);
         Workspace &w = *W;
         CUDA_OR_RETURN(w.x64.ensure(sizeof(double) * vec));
         CUDA_OR_RETURN(w.v0.ensure(sizeof(T) * vec));
         CUDA_OR_RETURN(w.v1.ensure(sizeof(T) * vec));
         CUDA_OR_RETURN(w.v2.ensure(sizeof(T) * vec));
         if (mixed) CUDA_OR_RETURN(w.v3.ensure(sizeof(float) * vec));
-        int ntmax = std::max(nt64, G->m32.g.ntiles);
-        for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, G->v32[v].g.ntiles);
+        int ntmax = std::max(nt64, nparts(G->m32));
+        for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, nparts(G->v32[v]));
         CUDA_OR_RETURN(w.apply_part.ensure(sizeof(double) * 2 * cap * ntmax));
         CUDA_OR_RETURN(w.res_part.ensure(sizeof(double) * 2 * cap * std::max(nt64, G->nchunks)));
         CUDA_OR_RETURN(w.rr_part.ensure(sizeof(double) * 2 * cap * G->nchunks));
@@ -1037,7 +1065,7 @@ struct SlotRun {
             CUDA_OR_RETURN((launch_march<double, T, MODE_RHS>(G, w.x64.as<double>(), w.v0.as<T>(), cs,
                                                                w.res_part.as<double>(), cap)));
             SolveParams sp2 = sp;
-            sp2.ntiles = G->m64.g.ntiles;
+            sp2.ntiles = nparts(G->m64);
             cg_true_residual_kernel<<<sb, 128, 0, G->stream>>>(st, sp2, w.res_part.as<double>(), cap, mixed, mask);
             launches += 2;
         } else {
@@ -1476,8 +1504,8 @@ static int profile_apply_impl(eqd_grid *G, int ncols, int warmup, int reps, doub
         int rc = tune_by_iterations(G, o, std::min(ncols, 1024));
         if (rc) return rc;
     }
-    int nt = G->m64.g.ntiles;
-    for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, G->v32[v].g.ntiles);
+    int nt = nparts(G->m64);
+    for (int v = 0; v < kNumVariants; ++v) nt = std::max(nt, nparts(G->v32[v]));
     CUDA_OR_RETURN(part.ensure(sizeof(double) * 2 * ncols * nt));
     fill_random_kernel<T><<<1184, 256, 0, G->stream>>>(x.as<T>(), n, 12345ull);
     CUDA_OR_RETURN(cudaGetLastError());

@@ -88,6 +88,10 @@ struct MarchGeom {
     long long colstride;
     int ntiles;            // x2 tiles per column
     int t2max;             // rows per tile (upper bound)
+    int nblk;              // x3 blocks of EQD_PBLK march steps: dot products are summed per
+                           // (column, tile, block), so any x3 segmentation gives the same bits
+    int nseg;              // x3 segments per (column, tile) in this launch
+    int segblk;            // blocks per segment
     int edge;              // > 0: the first and last tiles have `edge` rows and the
                            // tiles between split the rest evenly; 0: all balanced
     int CH;                // ring chunk capacity (elements) per (side, comp)
@@ -253,8 +257,17 @@ __global__ void __launch_bounds__(MAXT, 1)
 plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__ MarchGeom g,
                    const T *__restrict__ in, TO *__restrict__ out, ColumnSet cs,
                    double *__restrict__ partials, unsigned *__restrict__ err) {
-    const int grp = blockIdx.x / g.ntiles;
-    const int tile = blockIdx.x % g.ntiles;
+    // FP64-input instances (the FP64 solve, and the true residual of both
+    // precisions) sum their dot products per x3 step block and can split a
+    // column's march along x3; FP32 instances (the mixed-precision CG apply)
+    // sum per (column, tile) over the whole march.
+    constexpr bool SEG = sizeof(T) == 8;
+    // CTA -> (column group, x2 tile, x3 segment).
+    const int nseg = SEG ? g.nseg : 1;
+    const int per_grp = g.ntiles * nseg;
+    const int grp = blockIdx.x / per_grp;
+    const int tile = (blockIdx.x % per_grp) / nseg;
+    const int seg = SEG ? blockIdx.x % nseg : 0;
     // Columns of this CTA; an inactive lane (past the end, not active, or not
     // flagged) mirrors an active one's input and stores nothing.
     int colv[L];
@@ -277,6 +290,30 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
     const int n1 = N1 > 0 ? N1 : g.n1;
     const int n2 = g.n2, n3 = g.n3;
+    // x3 segment (FP64-input instances). March step s ingests plane s, does
+    // the in-plane work and finishes components 1, 2 of plane p = s - 3, and
+    // finishes component 3 of plane z = s - 6. Steps are grouped in blocks of
+    // EQD_PBLK: step s belongs to block min((s - 3) / EQD_PBLK, nblk - 1), and
+    // the dot-product contributions of a block's steps are summed together. A
+    // segment owns whole blocks [blk0, blk0 + nbs): steps [q0 + 3, q1 + 3)
+    // (the last segment: to n3 + 6), so it stores components 1, 2 of planes
+    // [q0, q1) and component 3 of planes [q0 - 3, q1 - 3). Before its first
+    // owned step it marches from plane q0 - 9 or earlier to fill the windows
+    // (z = q0 - 3 needs F3 of planes q0 - 6 .. q0, each from planes
+    // p - 3 .. p + 3); the start is a multiple of the ring depth, so plane q
+    // always uses ring slot q % EQD_NSLOT. FP32 instances march the whole
+    // column: steps [0, n3 + 6).
+    const int q0 = SEG ? seg * g.segblk * EQD_PBLK : 0;
+    const int q1 = SEG ? min(q0 + g.segblk * EQD_PBLK, n3) : n3;
+    const int blk0 = q0 / EQD_PBLK;
+    const int nbs = (q1 - q0 + EQD_PBLK - 1) / EQD_PBLK;   // blocks of this segment
+    const int o_beg = q0 + 3;                               // owned steps: [o_beg, s_end)
+    const int s_end = q1 == n3 ? n3 + 6 : q1 + 3;
+    const int s_beg = q0 > 9 ? (q0 - 9) / EQD_NSLOT * EQD_NSLOT : 0;
+    const unsigned ph0 = (unsigned)(s_beg / EQD_NSLOT) & 1u;  // mbarrier phase parity of plane s_beg
+    const int ing_end = min(n3, s_end);                     // planes ingested: [s_beg, ing_end)
+    const int p_lo = max(q0 - 6, 0);                        // in-plane work: p in [p_lo, p_hi)
+    const int p_hi = min(n3, s_end - 3);
     int a0, a1;
     if (g.edge > 0) {
         // Edge tiles hold every closure row (and read the 11 rows the wide
@@ -318,6 +355,11 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const int NP = N1 > 0 ? NPc : 2 * n1 * g.t2max;           // exchange entries per parity
     T *xF1 = ring + (size_t)L * RS;                           // [L][2 (step parity)][NP]
     T *xH21 = xF1 + (size_t)L * 2 * NP;                       // [L][2][NP]
+    // Per-(block, warp) dot-product sums (FP64-input instances):
+    // [L][segblk][warps][2].
+    const int nwarps = (int)(blockDim.x >> 5);
+    double *rblk = reinterpret_cast<double *>(
+        (reinterpret_cast<uintptr_t>(xH21 + (size_t)L * 2 * NP) + 15) & ~(uintptr_t)15);
 
     // ---- thread -> point: warp-homogeneous classes --------------------------
     // class 0: x2-interior rows, not on the fault; class 1: x2-closure rows,
@@ -376,6 +418,10 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     {
         const int nring = L * RS;
         for (int i = tid; i < nring; i += blockDim.x) ring[i] = T(0);
+        if constexpr (SEG) {
+            const int nrb = L * g.segblk * nwarps * 2;
+            for (int i = tid; i < nrb; i += blockDim.x) rblk[i] = 0.0;
+        }
         fence_proxy_async_smem();
         if (tid == 0) {
             for (int k = 0; k < EQD_NSLOT; ++k) mbar_init(&mbar[k], 1);
@@ -399,9 +445,9 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             }
         }
     };
-    int issued = min(EQD_NSLOT, n3);
+    int issued = min(s_beg + EQD_NSLOT, ing_end);  // planes [s_beg, issued) issued
     if (tid == 0) {
-        for (int q = 0; q < issued; ++q) issue_plane(q);
+        for (int q = s_beg; q < issued; ++q) issue_plane(q);
     }
 
     // Per-thread x1 row operators (start column within the line + 6 taps).
@@ -465,12 +511,32 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         for (int k = 0; k < 4; ++k) w3q[l][k] = T(0);
     }
 
+    // Dot-product sums (FP64-input instances: of the current step block,
+    // flushed per block).
     double acc0[L], acc1[L];
 #pragma unroll
     for (int l = 0; l < L; ++l) acc0[l] = acc1[l] = 0.0;
     const T lam = C.lam, mu = C.mu, lpm = C.lpm, sat = C.sat_c;
-    const int nsteps = n3 + 6;
     int dead_at = -1;
+    const int lane = tid & 31, warp = tid >> 5;
+    // Warp sums into this warp's slot of block b (all lanes take part).
+    auto flush = [&](int b) {
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            double x = acc0[l], y = acc1[l];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                x += __shfl_down_sync(0xffffffffu, x, o);
+                y += __shfl_down_sync(0xffffffffu, y, o);
+            }
+            if (lane == 0) {
+                double *slot = rblk + (((size_t)l * g.segblk + b) * nwarps + warp) * 2;
+                slot[0] += x;
+                slot[1] += y;
+            }
+            acc0[l] = acc1[l] = 0.0;
+        }
+    };
 
     // One march step. Windows are ordered by age: index 6 holds plane s,
     // index 3 plane p = s - 3; the F3 window holds p at 6 and z = s - 6 at 3;
@@ -480,7 +546,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         // ---- ingest plane s ----------------------------------------------------
         if (s < n3) {
             const int slot = s % EQD_NSLOT;
-            if (!mbar_wait_bounded(&mbar[slot], (unsigned)((s / EQD_NSLOT) & 1), err)) s_dead[buf] = 1;
+            if (!mbar_wait_bounded(&mbar[slot], ((unsigned)(s / EQD_NSLOT) & 1u) ^ ph0, err)) s_dead[buf] = 1;
             if (MODE != MODE_A) {
                 // Fix-up pass on the landed plane: chi (RHS) or P (generic input).
                 const int nrows = r1 - r0;
@@ -560,7 +626,9 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
 
         // ---- in-plane work at p = s - 3 ---------------------------------------
         const int p = s - 3;
-        const bool pin = p >= 0 && p < n3;
+        const bool pin = p >= p_lo && p < p_hi;
+        const bool owned = s >= o_beg;          // (s < s_end always)
+        const bool pout = owned && p < n3;      // components 1, 2 of plane p are stored here
         const bool x3i = p >= 4 && p <= n3 - 5;  // x3-interior plane (block-uniform)
         const int r3 = p < 4 ? p : 4 + (n3 - 1 - p);
         T w1[L], w2[L], w3p[L], F3[L];
@@ -664,13 +732,13 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             return false;
         }
         // Slot of plane p is free: every thread has passed its last read.
-        if (s >= 3 && s + 3 < n3) {
+        if (s - s_beg >= 3 && s + 3 < ing_end) {
             if (tid == 0) issue_plane(s + 3);
             issued = s + 4;
         }
 
         // ---- finish p: x1 derivatives of F1, H21; P, H; store -----------------
-        if (valid && pin) {
+        if (valid && pout) {
             const T hw = hpt * plane_weight(A3, p, n3);
 #pragma unroll
             for (int l = 0; l < L; ++l) {
@@ -709,7 +777,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         }
         // ---- finish z = s - 6: comp 3 --------------------------------------------
         const int z = s - 6;
-        if (valid && z >= 0 && z < n3) {
+        const bool zout = owned && z >= 0 && z < n3;
+        if (valid && zout) {
             const T hw = hpt * plane_weight(A3, z, n3);
             const bool x3iz = z >= 4 && z <= n3 - 5;
             const int r3z = z < 4 ? z : 4 + (n3 - 1 - z);
@@ -733,30 +802,61 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     };
 
     bool alive = true;
-    for (int s = 0; s < nsteps && alive; ++s) alive = step(s);
+    if constexpr (SEG) {
+        // Lead-in steps, then the owned step blocks, each closed by a flush
+        // (every lane of every warp takes part).
+        int s = s_beg;
+        for (; s < o_beg && alive; ++s) alive = step(s);
+        for (int b = blk0; b < blk0 + nbs && alive; ++b) {
+            const int e = b == g.nblk - 1 ? s_end : min(b * EQD_PBLK + 3 + EQD_PBLK, s_end);
+            for (; s < e && alive; ++s) alive = step(s);
+            if (alive) flush(b - blk0);
+        }
+    } else {
+        for (int s = 0; s < s_end && alive; ++s) alive = step(s);
+    }
 
     if (!alive) {
         // A wait gave up (recorded in *err). Before the CTA's shared memory is
         // released, wait (bounded) for every plane copy issued and not yet
         // consumed: planes dead_at .. issued-1.
         if (tid == 0) {
-            for (int q = max(dead_at, 0); q < issued; ++q)
-                mbar_wait_bounded(&mbar[q % EQD_NSLOT], (unsigned)((q / EQD_NSLOT) & 1), err);
+            for (int q = max(dead_at, s_beg); q < issued; ++q)
+                mbar_wait_bounded(&mbar[q % EQD_NSLOT], ((unsigned)(q / EQD_NSLOT) & 1u) ^ ph0, err);
         }
         __syncthreads();
         return;
     }
 
+    if constexpr (SEG) {
+        // Per (column, tile, step block): the warps' sums in warp order.
+        __syncthreads();
+        if (partials) {
 #pragma unroll
-    for (int l = 0; l < L; ++l) {
-        const double s0 = block_sum(acc0[l], red);
-        __syncthreads();
-        const double s1v = block_sum(acc1[l], red);
-        __syncthreads();
-        if (tid == 0 && partials && act[l]) {
-            double *pp = partials + ((long long)colv[l] * g.ntiles + tile) * 2;
-            pp[0] = s0;
-            pp[1] = s1v;
+            for (int l = 0; l < L; ++l) {
+                if (!act[l]) continue;
+                for (int i = tid; i < nbs * 2; i += blockDim.x) {
+                    const int k = i & 1, b = i >> 1;
+                    const double *src = rblk + ((size_t)l * g.segblk + b) * nwarps * 2 + k;
+                    double sum = 0.0;
+                    for (int w = 0; w < nwarps; ++w) sum += src[(size_t)w * 2];
+                    partials[(((long long)colv[l] * g.ntiles + tile) * g.nblk + blk0 + b) * 2 + k] = sum;
+                }
+            }
+        }
+    } else {
+        // Per (column, tile): block tree over the whole march.
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            const double s0 = block_sum(acc0[l], red);
+            __syncthreads();
+            const double s1v = block_sum(acc1[l], red);
+            __syncthreads();
+            if (tid == 0 && partials && act[l]) {
+                double *pp = partials + ((long long)colv[l] * g.ntiles + tile) * 2;
+                pp[0] = s0;
+                pp[1] = s1v;
+            }
         }
     }
 }

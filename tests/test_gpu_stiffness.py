@@ -165,6 +165,26 @@ def test_gemv(eqd):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_x3_segmented_equals_whole_columns(eqd, precision):
+    """Small batches split each column's stencil march along x3 (one column
+    here runs as 4 segments of 8 planes, 38 columns as 2 segments of 16);
+    338 columns run unsplit. The dot products are summed per block of 8
+    march steps whatever the split, so K columns and iteration counts are
+    the same bits."""
+    fe = eqd.FaultElasticity(eqd.cube_grids(25), LAM, MU, 0.5, precision=precision)   # 25^3 nodes, nf 169
+    eqd.set_stencil_variant(fe, 1)
+    cols = np.arange(2 * fe.nf)
+    Kb, itb, stb = eqd.stiffness_columns(fe, cols)
+    assert (stb == 1).all()
+    part = cols[::9][:40]
+    Km, itm, _ = eqd.stiffness_columns(fe, part)
+    assert np.array_equal(Km, Kb[:, part]) and np.array_equal(itm, itb[part])
+    for c in (0, fe.nf // 2, 2 * fe.nf - 1):
+        K1, it1, _ = eqd.stiffness_columns(fe, [c])
+        assert np.array_equal(K1[:, 0], Kb[:, c]) and it1[0] == itb[c]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_slot_refill_equals_full_batch(eqd, precision):
     """With fewer slots than columns, columns enter as earlier ones finish
     (continuous batching); every K column is bit-identical to the one built
