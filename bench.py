@@ -391,6 +391,7 @@ def main():
     nz = cols[np.abs(Kmix).sum(0) > 0]  # skip columns whose right-hand side is zero (ring nodes)
     sample = np.sort(rng.choice(nz, size=min(n_plain, len(nz)), replace=False)).astype(np.int32)
     eqd.stiffness_columns(plain, sample[:1])
+    eqd.stiffness_columns(plain, sample[-1:])
     t0 = time.perf_counter()
     lat = []
     for c in sample:
