@@ -124,7 +124,7 @@ class CGSolver:
     FP64 true residual."""
 
     def __init__(self, fe=None, rtol=1e-10, atol=0.0, itmax=0, precond="none", precision="mixed",
-                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0, split=True):
+                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0, split=True, fuse=False):
         if precond not in _PRECONDS:
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precond must be :none or :jacobi, got {precond}")
         if precision not in _PRECISIONS:
@@ -135,6 +135,7 @@ class CGSolver:
         self.chunk, self.reliable_delta = int(chunk), float(reliable_delta)
         self.hbm_budget_bytes, self.tile_rows = int(hbm_budget_bytes), int(tile_rows)
         self.split = bool(split)
+        self.fuse = bool(fuse)
         self.stats = CGStats()
         self._warned = False
 
@@ -149,6 +150,8 @@ class CGSolver:
         o.tile_rows = self.tile_rows
         if not self.split:
             o.flags |= _abi.EQD_FLAG_NO_SPLIT
+        if self.fuse:
+            o.flags |= _abi.EQD_FLAG_FUSE
         return o
 
     def record(self, st):
@@ -164,7 +167,8 @@ class CGSolver:
     def duplicate(self):
         """`duplicate(solver)`: same operator and options, fresh counters."""
         return CGSolver(self.fe, self.rtol, self.atol, self.itmax, self.precond, self.precision,
-                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.tile_rows, self.split)
+                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.tile_rows, self.split,
+                        self.fuse)
 
     def report(self):
         t = self.stats

@@ -41,6 +41,9 @@ struct ColumnSet {
     const int8_t *flag;        // per-column "do this step" flag (null: all)
     const double *dinv;        // MODE_RHS: Jacobi weights (one column, device layout) for
                                // the second partial sum(dinv y^2); null: none
+    const void *pold;          // MODE_AF: previous search direction (read), columns as the input
+    void *pnew;                // MODE_AF: new search direction r + beta p (written)
+    const double *beta;        // MODE_AF: per-column beta
 };
 
 enum ColStatus : int8_t {

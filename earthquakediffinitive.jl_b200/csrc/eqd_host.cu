@@ -70,6 +70,7 @@ struct MarchCfg {
     MarchGeom g;
     int threads = 0;
     size_t smem = 0;
+    size_t smem_af = 0;  // MODE_AF (second plane ring); 0: does not fit, the direction update runs apart
 };
 
 static constexpr int kMaxT32 = 640;   // generic FP32 instances
@@ -154,6 +155,8 @@ static bool make_march_cfg(int n1, int n2, int n3, int PS, long long colstride, 
     // exchange [2][points] x 2; FP64: per-(step block, warp) dot-product sums
     out.smem = 64 + 32 * 8 + (size_t)lanes * ((size_t)EQD_NSLOT * 6 * CH + 4 * (size_t)NP) * sizeof(T);
     if (sizeof(T) == 8) out.smem += 16 + (size_t)lanes * out.g.nblk * (threads / 32) * 2 * sizeof(double);
+    // MODE_AF adds the ring of r planes (aligned to 128 bytes after the rest).
+    out.smem_af = out.smem + 144 + (size_t)lanes * EQD_NSLOT * 6 * CH * sizeof(T);
     return true;
 }
 
@@ -221,6 +224,7 @@ struct Workspace {
     int cap = 0;            // columns
     int precision = -1;
     DevBuf x64, v0, v1, v2, v3;  // x64 + (r, p, q, d) in the working precision
+    DevBuf v4;                   // fused direction update: the other p buffer (p alternates v1, v4)
     DevBuf apply_part, res_part, rr_part;
     DevBuf gamma, beta, rr_ref, tol, bnorm, iters, status, flag;
     DevBuf slip_node, slip_comp, slip_dense;
@@ -230,6 +234,7 @@ struct Workspace {
     PinnedArr<double> kstage;             // finished K columns on their way to a host K
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
+    bool graph_split = false;  // the captured iterations run as two halves
     std::vector<uint64_t> graph_key;  // what the captured graph baked in (see SlotRun::setup)
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -306,27 +311,29 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
     cs.ncols = ncols;
     cudaStream_t st = stream ? stream : G->stream;
     const int n1 = G->gc.n1;
-    if (sizeof(T) == 4 && MODE == MODE_A) {
+    if constexpr (sizeof(T) == 4 && (MODE == MODE_A || MODE == MODE_AF)) {
         const int v = variant >= 0 ? variant : G->sel32;
         const int lanes = G->v32_lanes[v];
         const long long groups = (ncols + lanes - 1) / lanes;
-        const MarchCfg m = segmented(G->v32[v], groups, G->num_sms);
+        MarchCfg m = segmented(G->v32[v], groups, G->num_sms);
+        if (MODE == MODE_AF) m.smem = m.smem_af;
         dim3 grid((unsigned)(groups * m.g.ntiles * m.g.nseg));
         const float *fin = reinterpret_cast<const float *>(in);
         float *fout = reinterpret_cast<float *>(out);
         if (lanes == 2)
-            launch_n1<float, float, MODE_A, kMaxT32c, 2>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
-                                                          G->err.as<unsigned>());
+            launch_n1<float, float, MODE, kMaxT32c, 2>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
+                                                        G->err.as<unsigned>());
         else if (G->v32_maxt[v] == kMaxT32)
-            launch_n1<float, float, MODE_A, kMaxT32>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
-                                                     G->err.as<unsigned>());
+            launch_n1<float, float, MODE, kMaxT32>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
+                                                   G->err.as<unsigned>());
         else
-            launch_n1<float, float, MODE_A, kMaxT32b>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
-                                                      G->err.as<unsigned>());
+            launch_n1<float, float, MODE, kMaxT32b>(n1, grid, m, st, G->c32, fin, fout, cs, partials,
+                                                    G->err.as<unsigned>());
         return cudaGetLastError();
     }
     constexpr int MAXT = sizeof(T) == 4 ? kMaxT32 : kMaxT64;
-    const MarchCfg m = segmented(sizeof(T) == 4 ? G->m32 : G->m64, ncols, G->num_sms);
+    MarchCfg m = segmented(sizeof(T) == 4 ? G->m32 : G->m64, ncols, G->num_sms);
+    if (MODE == MODE_AF) m.smem = m.smem_af;
     const OpConst<T> &C = *reinterpret_cast<const OpConst<T> *>(sizeof(T) == 4 ? (const void *)&G->c32
                                                                                : (const void *)&G->c64);
     dim3 grid((unsigned)(ncols * m.g.ntiles * m.g.nseg));
@@ -358,7 +365,12 @@ static cudaError_t configure_kernels(int smem_max) {
         (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64, N, 1>,   \
         (const void *)plane_march_kernel<double, double, MODE_A, kMaxT64b, N, 1>,  \
         (const void *)plane_march_kernel<double, double, MODE_RHS, kMaxT64b, N, 1>, \
-        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64b, N, 1>,
+        (const void *)plane_march_kernel<double, float, MODE_RHS, kMaxT64b, N, 1>,       \
+        (const void *)plane_march_kernel<float, float, MODE_AF, kMaxT32, N, 1>,          \
+        (const void *)plane_march_kernel<float, float, MODE_AF, kMaxT32b, N, 1>,         \
+        (const void *)plane_march_kernel<float, float, MODE_AF, kMaxT32c, N, 2>,         \
+        (const void *)plane_march_kernel<double, double, MODE_AF, kMaxT64, N, 1>,        \
+        (const void *)plane_march_kernel<double, double, MODE_AF, kMaxT64b, N, 1>,
     const void *ks[] = {
         EQD_FOR_N1(EQD_KS) EQD_KS(0)
         (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32, 0, 1>,
@@ -523,6 +535,12 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
         for (int v = 0; v < kNumVariants; ++v) need = std::max(need, G->v32[v].smem);
         if ((size_t)optin < need)
             return fail(EQD_ERR_ARG, "stencil tile needs more shared memory than the device offers");
+        // A configuration whose second ring does not fit runs the direction
+        // update as its own kernel.
+        for (MarchCfg *m : {&G->m32, &G->m64})
+            if (m->smem_af > (size_t)optin) m->smem_af = 0;
+        for (int v = 0; v < kNumVariants; ++v)
+            if (G->v32[v].smem_af > (size_t)optin) G->v32[v].smem_af = 0;
         // The limit is a per-kernel attribute shared by every grid of the
         // process: set it to the device maximum, once per device.
         CUDA_OR_RETURN(configure_kernels(optin));
@@ -664,7 +682,9 @@ struct BatchSpec {
 
 static int resolve_chunk(eqd_grid *G, const eqd_solve_opts &o, int ncols, int prec, int &chunk) {
     const GridConst &gc = G->gc;
-    const size_t per_col = (size_t)gc.colstride * (prec == EQD_PREC_MIXED ? (8 + 4 * 4) : (8 + 3 * 8)) +
+    // x64 + r, p, q (+ d) (+ the second direction buffer of the fused update).
+    const int nvec = 3 + (prec == EQD_PREC_MIXED ? 1 : 0) + ((o.flags & EQD_FLAG_FUSE) ? 1 : 0);
+    const size_t per_col = (size_t)gc.colstride * (8 + (size_t)nvec * (prec == EQD_PREC_MIXED ? 4 : 8)) +
                            (size_t)16 * gc.nf + 1024;
     size_t budget = o.hbm_budget_bytes;
     if (budget == 0) {
@@ -693,6 +713,7 @@ struct IterPtrs {
     ColumnSet cs;
     ColState st;
     T *r, *p, *q;
+    T *p2;  // fused direction update: the other direction buffer
     float *d;
     double *x64, *apply_part, *res_part, *rr_part;
 };
@@ -712,6 +733,7 @@ static IterPtrs<T> span_ptrs(eqd_grid *G, Workspace &W, const SolveParams &sp, c
     P.r = W.v0.as<T>() + c0 * gc.colstride;
     P.p = W.v1.as<T>() + c0 * gc.colstride;
     P.q = W.v2.as<T>() + c0 * gc.colstride;
+    P.p2 = W.v4.p ? W.v4.as<T>() + c0 * gc.colstride : nullptr;
     P.d = W.v3.p ? W.v3.as<float>() + c0 * gc.colstride : nullptr;
     P.x64 = W.x64.as<double>() + c0 * gc.colstride;
     P.apply_part = W.apply_part.as<double>() + c0 * sp.ntiles * 2;
@@ -720,15 +742,32 @@ static IterPtrs<T> span_ptrs(eqd_grid *G, Workspace &W, const SolveParams &sp, c
     return P;
 }
 
-// The stencil apply of one CG iteration (q = A p, partial p.q).
+// The direction of iteration k when the direction update is fused into the
+// apply: iteration k reads the previous direction from one buffer and writes
+// the new one to the other (v1 at even k, v4 at odd k; kIter is even, so a
+// graph launch always starts with the current direction in v1).
 template <typename T>
-static void record_apply(eqd_grid *G, Workspace &W, int generic, const SolveParams &sp, const ColState &st0,
-                         const Span &sn) {
+static T *dir_in(const IterPtrs<T> &P, int k) { return (k & 1) ? P.p2 : P.p; }
+template <typename T>
+static T *dir_out(const IterPtrs<T> &P, int k) { return (k & 1) ? P.p : P.p2; }
+
+// The stencil apply of CG iteration k (q = A p, partial p.q); fused: with
+// p = r + beta p formed on the way in.
+template <typename T>
+static void record_apply(eqd_grid *G, Workspace &W, int generic, int fused, int k, const SolveParams &sp,
+                         const ColState &st0, const Span &sn) {
     IterPtrs<T> P = span_ptrs<T>(G, W, sp, st0, sn);
-    if (generic)
+    if (generic) {
         launch_march<T, T, MODE_AP>(G, P.p, P.q, P.cs, P.apply_part, sn.n, -1, sn.s);
-    else
+    } else if (fused) {
+        ColumnSet cs = P.cs;
+        cs.pold = dir_in(P, k);
+        cs.pnew = dir_out(P, k);
+        cs.beta = P.st.beta;
+        launch_march<T, T, MODE_AF>(G, P.r, P.q, cs, P.apply_part, sn.n, -1, sn.s);
+    } else {
         launch_march<T, T, MODE_A>(G, P.p, P.q, P.cs, P.apply_part, sn.n, -1, sn.s);
+    }
 }
 
 // CTA size of the vector kernels inside the iterations: small enough
@@ -741,12 +780,13 @@ static constexpr int kVecThreads = 128;
 // gave 6.0, 6.6, 6.5, 6.3 k columns/s; one chain with one CTA per item 6.2 k).
 static constexpr int kVecCtasPerSm = 4;
 
-// The rest of the iteration: x, r updates; scalars; reliable update (mixed);
-// the next direction.
+// The rest of iteration k: x, r updates; scalars; reliable update (mixed);
+// the next direction (unless the next apply forms it).
 template <typename T>
-static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams &sp, const ColState &st0,
-                        const Span &sn) {
+static void record_rest(eqd_grid *G, Workspace &W, int mixed, int fused, int k, const SolveParams &sp,
+                        const ColState &st0, const Span &sn) {
     IterPtrs<T> P = span_ptrs<T>(G, W, sp, st0, sn);
+    const T *pk = fused ? dir_out(P, k) : P.p;  // this iteration's direction
     const int nch = G->nchunks;
     const double *dinv64 = sp.precond ? G->dinv64.as<double>() : nullptr;
     const float *dinv32 = sp.precond ? G->dinv32.as<float>() : nullptr;
@@ -755,11 +795,11 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
     const long long items = (long long)sn.n * nch;
     const unsigned nb = (unsigned)(sn.split ? std::min<long long>(items, (long long)G->num_sms * kVecCtasPerSm) : items);
     if (mixed) {
-        cg_update_kernel<float, float><<<nb, kVecThreads, 0, sn.s>>>(P.d, (float *)P.r, (const float *)P.p,
+        cg_update_kernel<float, float><<<nb, kVecThreads, 0, sn.s>>>(P.d, (float *)P.r, (const float *)pk,
                                                             (const float *)P.q, P.apply_part, P.st, sp, P.rr_part,
                                                             dinv32, sn.n);
     } else {
-        cg_update_kernel<double, double><<<nb, kVecThreads, 0, sn.s>>>(P.x64, (double *)P.r, (const double *)P.p,
+        cg_update_kernel<double, double><<<nb, kVecThreads, 0, sn.s>>>(P.x64, (double *)P.r, (const double *)pk,
                                                               (const double *)P.q, P.apply_part, P.st, sp,
                                                               P.rr_part, dinv64, sn.n);
     }
@@ -777,8 +817,10 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
         sp2.ntiles = nparts(G->m64);
         cg_true_residual_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp2, P.res_part, sn.n, 1);
     }
-    const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
-    cg_pupdate_kernel<T><<<nb, kVecThreads, 0, sn.s>>>(P.p, P.r, P.st, sp, nullptr, dinvT, sn.n);
+    if (!fused) {
+        const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
+        cg_pupdate_kernel<T><<<nb, kVecThreads, 0, sn.s>>>(P.p, P.r, P.st, sp, nullptr, dinvT, sn.n);
+    }
 }
 
 // Capture kIter CG iterations over `cap` slots. Large batches are split in
@@ -786,13 +828,13 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, const SolveParams 
 // arithmetic-bound apply of one half runs while the memory-bound vector
 // updates of the other half stream through HBM.
 template <typename T>
-static void record_iterations(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, const SolveParams &sp,
-                              const ColState &st, int kIter, bool split) {
+static void record_iterations(eqd_grid *G, Workspace &W, int cap, int mixed, int generic, int fused,
+                              const SolveParams &sp, const ColState &st, int kIter, bool split) {
     if (!split) {
         const Span all{0, cap, G->stream, false};
         for (int k = 0; k < kIter; ++k) {
-            record_apply<T>(G, W, generic, sp, st, all);
-            record_rest<T>(G, W, mixed, sp, st, all);
+            record_apply<T>(G, W, generic, fused, k, sp, st, all);
+            record_rest<T>(G, W, mixed, fused, k, sp, st, all);
         }
         return;
     }
@@ -809,17 +851,17 @@ static void record_iterations(eqd_grid *G, Workspace &W, int cap, int mixed, int
             cudaStreamWaitEvent(A.s, G->evB, 0);      // B's previous apply is done
             cudaStreamWaitEvent(A.s, G->evArest, 0);  // A's previous direction is ready
         }
-        record_apply<T>(G, W, generic, sp, st, A);
+        record_apply<T>(G, W, generic, fused, k, sp, st, A);
         cudaEventRecord(G->evA, A.s);
         cudaStreamWaitEvent(B.s, G->evA, 0);          // B's apply follows A's
         if (k > 0) cudaStreamWaitEvent(B.s, G->evBrest, 0);
-        record_apply<T>(G, W, generic, sp, st, B);
+        record_apply<T>(G, W, generic, fused, k, sp, st, B);
         cudaEventRecord(G->evB, B.s);
         cudaStreamWaitEvent(Ah.s, G->evA, 0);
-        record_rest<T>(G, W, mixed, sp, st, Ah);
+        record_rest<T>(G, W, mixed, fused, k, sp, st, Ah);
         cudaEventRecord(G->evArest, Ah.s);
         cudaStreamWaitEvent(Bh.s, G->evB, 0);
-        record_rest<T>(G, W, mixed, sp, st, Bh);
+        record_rest<T>(G, W, mixed, fused, k, sp, st, Bh);
         cudaEventRecord(G->evBrest, Bh.s);
     }
     cudaEventRecord(G->evJoin, B.s);
@@ -884,6 +926,7 @@ struct SlotRun {
     eqd_grid *G = nullptr;
     Workspace *W = nullptr;
     int cap = 0, mixed = 0, generic = 0, dense = 0;
+    int fused = 0;  // the direction update runs inside the stencil apply (MODE_AF)
     long long itmax = 0;
     SolveParams sp{};
     ColState st{};
@@ -917,6 +960,12 @@ struct SlotRun {
         CUDA_OR_RETURN(w.v1.ensure(sizeof(T) * vec));
         CUDA_OR_RETURN(w.v2.ensure(sizeof(T) * vec));
         if (mixed) CUDA_OR_RETURN(w.v3.ensure(sizeof(float) * vec));
+        {
+            const MarchCfg &mc = sizeof(T) == 4 ? G->v32[G->sel32] : G->m64;
+            fused = !generic && o.precond != EQD_PRECOND_JACOBI && (o.flags & EQD_FLAG_FUSE) && mc.smem_af > 0;
+        }
+        if (fused) CUDA_OR_RETURN(w.v4.ensure(sizeof(T) * vec));
+        else w.v4.release();
         int ntmax = std::max(nt64, nparts(G->m32));
         for (int v = 0; v < kNumVariants; ++v) ntmax = std::max(ntmax, nparts(G->v32[v]));
         CUDA_OR_RETURN(w.apply_part.ensure(sizeof(double) * 2 * cap * ntmax));
@@ -975,13 +1024,13 @@ struct SlotRun {
         // workspace pointer (a buffer that grew or was released since the
         // capture must not be reached through the old graph).
         std::vector<uint64_t> kv = {(uint64_t)cap, (uint64_t)o.precision, (uint64_t)generic, (uint64_t)G->sel32,
-                                    (uint64_t)o.precond, (uint64_t)split, (uint64_t)sp.itmax};
+                                    (uint64_t)o.precond, (uint64_t)split, (uint64_t)sp.itmax, (uint64_t)fused};
         for (double d : {sp.rtol, sp.atol, sp.delta}) {
             uint64_t b;
             std::memcpy(&b, &d, sizeof(b));
             kv.push_back(b);
         }
-        for (const void *q : {w.x64.p, w.v0.p, w.v1.p, w.v2.p, w.v3.p, w.apply_part.p, w.res_part.p, w.rr_part.p,
+        for (const void *q : {w.x64.p, w.v0.p, w.v1.p, w.v2.p, w.v3.p, w.v4.p, w.apply_part.p, w.res_part.p, w.rr_part.p,
                               w.gamma.p, w.beta.p, w.rr_ref.p, w.tol.p, w.bnorm.p, w.iters.p, w.status.p, w.flag.p,
                               w.slip_node.p, w.slip_comp.p, w.slip_dense.p, G->dinv64.p, G->dinv32.p})
             kv.push_back((uint64_t)(uintptr_t)q);
@@ -990,7 +1039,7 @@ struct SlotRun {
             w.graph = nullptr;
             cudaGraph_t g;
             CUDA_OR_RETURN(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
-            record_iterations<T>(G, w, cap, mixed, generic, sp, st, kIter, split);
+            record_iterations<T>(G, w, cap, mixed, generic, fused, sp, st, kIter, split);
             cudaError_t ce = cudaStreamEndCapture(G->stream, &g);
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
             ce = cudaGraphInstantiate(&w.graph, g, cudaGraphInstantiateFlagUseNodePriority);
@@ -998,6 +1047,7 @@ struct SlotRun {
             if (ce != cudaSuccess) return fail(EQD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
             w.graph_key = kv;
             w.graph_iters = kIter;
+            w.graph_split = split;
         }
         return EQD_OK;
     }
@@ -1055,7 +1105,9 @@ struct SlotRun {
         zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v1.as<T>(), cst, G->nchunks, mask);
         zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v2.as<T>(), cst, G->nchunks, mask);
         if (mixed) zero_columns_kernel<float><<<nb, 256, 0, G->stream>>>(w.v3.as<float>(), cst, G->nchunks, mask);
-        launches += mixed ? 5 : 4;
+        // Fused: the second direction buffer's plane padding must read as zero.
+        if (fused) zero_columns_kernel<T><<<nb, 256, 0, G->stream>>>(w.v4.as<T>(), cst, G->nchunks, mask);
+        launches += (mixed ? 5 : 4) + (fused ? 1 : 0);
         const unsigned sb = (unsigned)((cap + 127) / 128);
         if (!generic) {
             // r0 = b = H P (D+SAT) chi  (x = 0), in the working precision.
@@ -1106,7 +1158,7 @@ struct SlotRun {
         for (int s = 0; s < cap; ++s) running += tag[s] >= 0 && hst[s] == COL_ACTIVE;
         if (running > 0) {
             CUDA_OR_RETURN(cudaGraphLaunch(w.graph, G->stream));
-            launches += (int64_t)kIter * (mixed ? 7 : 4);
+            launches += (int64_t)kIter * ((mixed ? 7 : 4) - (fused ? 1 : 0)) * (w.graph_split ? 2 : 1);
         }
         CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), w.status.p, cap, cudaMemcpyDeviceToHost, G->stream));
         CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), w.iters.p, sizeof(int) * cap, cudaMemcpyDeviceToHost, G->stream));
@@ -1925,7 +1977,8 @@ extern "C" int eqd_server_add_grid(eqd_server *S, eqd_grid *G, int32_t slots) {
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
     const GridConst &gc = G->gc;
     const int mixed = S->opts.precision == EQD_PREC_MIXED;
-    const size_t per_slot = (size_t)gc.colstride * (mixed ? (8 + 4 * 4) : (8 + 3 * 8)) + (size_t)16 * gc.nf + 1024;
+    const int nvec = 3 + (mixed ? 1 : 0) + ((S->opts.flags & EQD_FLAG_FUSE) ? 1 : 0);
+    const size_t per_slot = (size_t)gc.colstride * (8 + (size_t)nvec * (mixed ? 4 : 8)) + (size_t)16 * gc.nf + 1024;
     std::unique_ptr<SrvGrid> g(new SrvGrid());
     {
         std::lock_guard<std::mutex> lk(S->mu);

@@ -5,6 +5,10 @@
 //   MODE_AP  : y = -H P (D + SAT) P x        (generic x; P applied in smem)
 //   MODE_RHS : y = +H P (D + SAT) (x + chi)  (x in range(P); chi from the
 //              column's slip) = b - A x, the true residual of the CG system
+//   MODE_AF  : p' = r + beta p, y = -H P (D + SAT) p'  (the CG direction
+//              update fused into the apply: r and p arrive by bulk copies,
+//              p' is formed on the landed planes in shared memory and
+//              written back; the input pointer is r)
 // where, per side, D is the constant-coefficient Navier operator
 //   (D v)_j = mu * sum_a D2_a v_j + mu * D2_j v_j + lam * D1_j D1_j v_j
 //             + (lam + mu) * sum_{k != j} D1_j D1_k v_k
@@ -44,7 +48,7 @@
 
 namespace eqd {
 
-enum { MODE_A = 0, MODE_AP = 1, MODE_RHS = 2 };
+enum { MODE_A = 0, MODE_AP = 1, MODE_RHS = 2, MODE_AF = 3 };
 
 // Per-axis operator tables, built on the host from the exact 1D matrices of
 // that axis length (so overlapping closures of short axes are exact).
@@ -360,6 +364,11 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     const int nwarps = (int)(blockDim.x >> 5);
     double *rblk = reinterpret_cast<double *>(
         (reinterpret_cast<uintptr_t>(xH21 + (size_t)L * 2 * NP) + 15) & ~(uintptr_t)15);
+    // MODE_AF: ring of the r planes, [L][slot][side*3+comp][CH], beside the
+    // ring of p planes (128-byte aligned, after the block sums).
+    T *rring = reinterpret_cast<T *>(
+        (reinterpret_cast<uintptr_t>(rblk) + (SEG ? (size_t)L * g.nblk * nwarps * 2 * sizeof(double) : 0) + 127) &
+        ~(uintptr_t)127);
 
     // ---- thread -> point: warp-homogeneous classes --------------------------
     // class 0: x2-interior rows, not on the fault; class 1: x2-closure rows,
@@ -418,6 +427,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     {
         const int nring = L * RS;
         for (int i = tid; i < nring; i += blockDim.x) ring[i] = T(0);
+        if constexpr (MODE == MODE_AF)
+            for (int i = tid; i < nring; i += blockDim.x) rring[i] = T(0);
         if constexpr (SEG) {
             const int nrb = L * g.segblk * nwarps * 2;
             for (int i = tid; i < nrb; i += blockDim.x) rblk[i] = 0.0;
@@ -432,22 +443,65 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
     }
     __syncthreads();
 
+    // MODE_AF: the p planes go to `ring` (where p' is formed) and the r
+    // planes to `rring`, both completing on the slot's mbarrier.
     auto issue_plane = [&](int q) {
         const int slot = q % EQD_NSLOT;
-        mbar_arrive_expect_tx(&mbar[slot], (unsigned)L * 6u * bytes);
+        mbar_arrive_expect_tx(&mbar[slot], (unsigned)L * (MODE == MODE_AF ? 12u : 6u) * bytes);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const T *incol = in + (long long)colv[l] * g.colstride;
+            const T *incol = (MODE == MODE_AF ? reinterpret_cast<const T *>(cs.pold) : in) + (long long)colv[l] * g.colstride;
             for (int sc = 0; sc < 6; ++sc) {
                 T *dst = ring + (size_t)l * RS + ((size_t)slot * 6 + sc) * CH + (e0 - base);
                 const T *src = incol + ((long long)sc * n3 + q) * g.PS + e0;
                 bulk_g2s(dst, src, bytes, &mbar[slot]);
             }
+            if constexpr (MODE == MODE_AF) {
+                const T *rcol = in + (long long)colv[l] * g.colstride;
+                for (int sc = 0; sc < 6; ++sc) {
+                    T *dst = rring + (size_t)l * RS + ((size_t)slot * 6 + sc) * CH + (e0 - base);
+                    const T *src = rcol + ((long long)sc * n3 + q) * g.PS + e0;
+                    bulk_g2s(dst, src, bytes, &mbar[slot]);
+                }
+            }
         }
+    };
+    // MODE_AF: p' = r + beta p on landed plane q (every thread; the caller
+    // orders it before the plane's readers with a CTA barrier). The same
+    // expression as the unfused direction update, so the same bits.
+    T beta_l[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) beta_l[l] = MODE == MODE_AF ? (T)cs.beta[colv[l]] : T(0);
+    const int nel = (int)(bytes / sizeof(T));
+    auto form_direction = [&](int q) {
+        T *p0 = ring + (size_t)(q % EQD_NSLOT) * 6 * CH + (e0 - base);
+        const long long roff = rring - ring;
+        for (int j = tid; j < nel; j += blockDim.x) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                T *pp = p0 + (size_t)l * RS + j;
+                const T *rp = pp + roff;
+#pragma unroll
+                for (int sc = 0; sc < 6; ++sc) pp[sc * CH] = rp[sc * CH] + beta_l[l] * pp[sc * CH];
+            }
+        }
+        // The slot is refilled by bulk copies later: order these generic-proxy
+        // writes before them.
+        fence_proxy_async_smem();
     };
     int issued = min(s_beg + EQD_NSLOT, ing_end);  // planes [s_beg, issued) issued
     if (tid == 0) {
         for (int q = s_beg; q < issued; ++q) issue_plane(q);
+    }
+    bool lead_ok = true;
+    if constexpr (MODE == MODE_AF) {
+        // The first plane's direction; each step then forms the next plane's
+        // before its barrier.
+        if (s_beg < ing_end) {
+            lead_ok = mbar_wait_bounded(&mbar[s_beg % EQD_NSLOT], ((unsigned)(s_beg / EQD_NSLOT) & 1u) ^ ph0, err);
+            if (lead_ok) form_direction(s_beg);
+        }
+        lead_ok = __syncthreads_and(lead_ok);
     }
 
     // Per-thread x1 row operators (start column within the line + 6 taps).
@@ -547,7 +601,7 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         if (s < n3) {
             const int slot = s % EQD_NSLOT;
             if (!mbar_wait_bounded(&mbar[slot], ((unsigned)(s / EQD_NSLOT) & 1u) ^ ph0, err)) s_dead[buf] = 1;
-            if (MODE != MODE_A) {
+            if (MODE == MODE_RHS || MODE == MODE_AP) {
                 // Fix-up pass on the landed plane: chi (RHS) or P (generic input).
                 const int nrows = r1 - r0;
 #pragma unroll
@@ -608,6 +662,16 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
                     c = c3[0];
                     h = x2_d1i(A2, c3, n1);
                     if (x2cl) x2_corr_d1(A2, gdd, c3, h);
+                    if constexpr (MODE == MODE_AF) {
+                        // The new direction of this CTA's own points and planes.
+                        if (act[l] && s >= q0 && s < q1) {
+                            T *pn = reinterpret_cast<T *>(cs.pnew) + (long long)colv[l] * g.colstride + poff +
+                                    (long long)s * g.PS;
+                            pn[0] = a;
+                            pn[cstr] = b;
+                            pn[2 * cstr] = c;
+                        }
+                    }
                 }
                 push7(v1w[l], a);
                 push7(v2w[l], b);
@@ -726,6 +790,16 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
             for (int k = 0; k < 3; ++k) w3q[l][k] = w3q[l][k + 1];
             w3q[l][3] = w3p[l];
         }
+        if constexpr (MODE == MODE_AF) {
+            // The next plane's direction, before the barrier that precedes its
+            // ingest (its slot is not read during this step).
+            if (s + 1 < ing_end) {
+                if (mbar_wait_bounded(&mbar[(s + 1) % EQD_NSLOT], ((unsigned)((s + 1) / EQD_NSLOT) & 1u) ^ ph0, err))
+                    form_direction(s + 1);
+                else
+                    s_dead[buf] = 1;
+            }
+        }
         __syncthreads();
         if (s_dead[buf]) {
             dead_at = s;
@@ -801,7 +875,8 @@ plane_march_kernel(const __grid_constant__ OpConst<T> C, const __grid_constant__
         return true;
     };
 
-    bool alive = true;
+    bool alive = lead_ok;
+    if (!alive) dead_at = s_beg;
     if constexpr (SEG) {
         // Lead-in steps, then the owned step blocks, each closed by a flush
         // (every lane of every warp takes part).

@@ -61,6 +61,11 @@ typedef enum { EQD_PRECOND_NONE = 0, EQD_PRECOND_JACOBI = 1 } eqd_precond;
 #define EQD_FLAG_STRICT 1u    /* return EQD_ERR_NOT_CONVERGED if any column did not converge */
 #define EQD_FLAG_NO_SPLIT 2u  /* run a large batch as one chain of kernels instead of two halves whose
                                  stencil applies alternate (for comparisons; results are identical) */
+#define EQD_FLAG_FUSE 4u      /* form the CG direction p = r + beta p inside the stencil apply (from bulk
+                                 copies of r and the previous p) instead of in its own kernel; results
+                                 are identical. Off by default: the apply is instruction-issue bound,
+                                 and the extra work there costs more than the separate memory-bound
+                                 kernel, which overlaps the other half's apply. */
 
 /*
  * Two equidistant blocks meeting at the fault plane x1 = 0:

@@ -166,11 +166,12 @@ def test_gemv(eqd):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_x3_segmented_equals_whole_columns(eqd, precision):
-    """Small batches split each column's stencil march along x3 (one column
-    here runs as 4 segments of 8 planes, 38 columns as 2 segments of 16);
-    338 columns run unsplit. The dot products are summed per block of 8
-    march steps whatever the split, so K columns and iteration counts are
-    the same bits."""
+    """FP64-input stencil launches (the FP64 CG apply; the true residual of
+    both precisions) of small batches split each column's march along x3
+    (one column here runs as 4 segments of 8 planes, 38 columns as 2
+    segments of 16); 338 columns run unsplit. The dot products are summed
+    per block of 8 march steps whatever the split, so K columns and
+    iteration counts are the same bits."""
     fe = eqd.FaultElasticity(eqd.cube_grids(25), LAM, MU, 0.5, precision=precision)   # 25^3 nodes, nf 169
     eqd.set_stencil_variant(fe, 1)
     cols = np.arange(2 * fe.nf)
@@ -182,6 +183,27 @@ def test_x3_segmented_equals_whole_columns(eqd, precision):
     for c in (0, fe.nf // 2, 2 * fe.nf - 1):
         K1, it1, _ = eqd.stiffness_columns(fe, [c])
         assert np.array_equal(K1[:, 0], Kb[:, c]) and it1[0] == itb[c]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("variant", [1, 3])
+def test_fused_direction_update_equals_separate(eqd, precision, variant):
+    """The CG direction p = r + beta p formed inside the stencil apply (from
+    bulk copies of r and the previous p; opt-in) gives the same bits as the
+    separate direction kernel: same K columns, same iteration counts.
+    Variant 3 runs two columns per thread."""
+    kw = dict(precision=precision)
+    fe_f = eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.6, fuse=True, **kw)
+    fe_u = eqd.FaultElasticity(eqd.cube_grids(13, L=1.2), LAM, MU, 0.6, **kw)
+    for fe in (fe_f, fe_u):
+        eqd.set_stencil_variant(fe, variant)
+    cols = np.arange(2 * fe_f.nf)
+    Kf, itf, stf = eqd.stiffness_columns(fe_f, cols)
+    Ku, itu, stu = eqd.stiffness_columns(fe_u, cols)
+    assert (stf == 1).all()
+    assert np.array_equal(Kf, Ku) and np.array_equal(itf, itu)
+    K1, it1, _ = eqd.stiffness_columns(fe_f, [5])      # one column alone, fused
+    assert np.array_equal(K1[:, 0], Ku[:, 5]) and it1[0] == itu[5]
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
