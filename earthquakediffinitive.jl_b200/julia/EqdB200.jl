@@ -26,6 +26,11 @@ struct GridDesc
     order::Int32; device::Int32
 end
 
+# SolveOpts.flags bits (include/eqd.h)
+const EQD_FLAG_STRICT = UInt32(1)    # return an error if a column did not converge
+const EQD_FLAG_NO_SPLIT = UInt32(2)  # one chain of kernels instead of two overlapping halves
+const EQD_FLAG_FUSE = UInt32(4)      # form the CG direction inside the stencil apply
+
 mutable struct SolveOpts
     rtol::Float64; atol::Float64; itmax::Int64
     precond::Int32; precision::Int32; chunk::Int32

@@ -84,3 +84,16 @@ def test_bad_arguments_rejected_without_gpu(built):
         eqd.build_model(dz=100.0, L_fault=800.0, L_normal=400.0)   # n1 = 5 < 9 (src/BP8.jl:198-204)
     with pytest.raises(ValueError):
         eqd.build_model(dz=30.0)   # does not divide l_f
+
+
+def test_flag_constants_match_header():
+    """The Python and Julia bindings' opts.flags bits are the header's."""
+    txt = open(HEADER).read()
+    hdr = {k: int(v) for k, v in re.findall(r"#define (EQD_FLAG_[A-Z_]+) (\d+)u", txt)}
+    assert set(hdr) == {"EQD_FLAG_STRICT", "EQD_FLAG_NO_SPLIT", "EQD_FLAG_FUSE"}
+    eqd = load_package()
+    for k, v in hdr.items():
+        assert getattr(eqd._abi, k) == v
+    jl = open(os.path.join(ROOT, "earthquakediffinitive.jl_b200", "julia", "EqdB200.jl")).read()
+    for k, v in hdr.items():
+        assert re.search(rf"const {k} = UInt32\({v}\)", jl), k
