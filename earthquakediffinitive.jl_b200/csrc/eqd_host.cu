@@ -770,9 +770,11 @@ static void record_apply(eqd_grid *G, Workspace &W, int generic, int fused, int 
     }
 }
 
-// CTA size of the vector kernels inside the iterations: small enough
-// (128 threads x 32 registers) to fit beside two resident stencil CTAs on an
-// SM, so the other half's updates can run while an apply is in flight.
+// CTA size of the vector kernels inside the iterations: small enough to fit
+// beside resident stencil CTAs on an SM (the update kernel's 128 threads x
+// 62-70 registers take the 8 K registers that two 224-thread, 128-register
+// stencil CTAs leave free), so the other half's updates can run while an
+// apply is in flight.
 static constexpr int kVecThreads = 128;
 // With a split batch the vector kernels run on 4 CTAs per SM (grid-stride):
 // they fit beside the other half's stencil CTAs and still stream at close to
