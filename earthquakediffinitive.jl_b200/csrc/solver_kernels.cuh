@@ -32,13 +32,26 @@ struct SolveParams {
     int precond;        // 1: Jacobi (gamma = r.z, z = dinv r); 0: none (z = r)
 };
 
+// 16-byte group of vector elements: the CG vector kernels move whole groups
+// (a column's storage is a multiple of 4 elements, its start 16-byte
+// aligned), two groups of every vector per thread per pass. Beside the
+// other half's stencil CTAs an SM has room for one 128-thread vector CTA
+// (at most 64 registers a thread), so the bytes each thread keeps in flight
+// set the memory parallelism the updates get there.
+template <typename T>
+struct alignas(16) Group {
+    static constexpr int N = 16 / (int)sizeof(T);
+    T v[N];
+};
+
 // ---------------------------------------------------------------------------
 // x += alpha p ; r -= alpha q ; partial r.r   (alpha = gamma / p.q)
 // X is the solution accumulator (FP64 for plain CG, FP32 correction d for the
 // mixed inner solve).
 // ---------------------------------------------------------------------------
 // rr_part[col][chunk][2] = (r.r, r.z) partials; r.z = r.r without a
-// preconditioner (`dinv` null), z = dinv r with one (Jacobi).
+// preconditioner (`dinv` null), z = dinv r with one (Jacobi). A chunk is a
+// contiguous range of 16-byte groups of the column.
 // Grid-stride over (column, chunk) items: any grid size gives the same
 // per-item partial sums, so a small grid (a few CTAs per SM, able to run
 // beside the stencil apply) is as exact as one CTA per item.
@@ -48,6 +61,10 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
                                                         const double *__restrict__ apply_part, ColState st,
                                                         SolveParams sp, double *__restrict__ rr_part,
                                                         const T *__restrict__ dinv, int ncols) {
+    static_assert(sizeof(T) == sizeof(TX), "x and r share the group layout");
+    using G = Group<T>;
+    using GX = Group<TX>;
+    constexpr int V = G::N;
     __shared__ double red[32];
     __shared__ double s_alpha;
     const int nitems = ncols * sp.nchunks;
@@ -67,42 +84,45 @@ __global__ void __launch_bounds__(256) cg_update_kernel(TX *__restrict__ x, T *_
         }
         __syncthreads();
         const double alpha = s_alpha;
-        const long long n = sp.colstride;
-        const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
-        const long long off = (long long)col * n;
+        const long long ng = sp.colstride / V;
+        const long long gbeg = ng * chunk / sp.nchunks, gend = ng * (chunk + 1) / sp.nchunks;
+        const long long off = (long long)col * sp.colstride;
+        GX *xg = reinterpret_cast<GX *>(x + off);
+        G *rg = reinterpret_cast<G *>(r + off);
+        const G *pg = reinterpret_cast<const G *>(p + off);
+        const G *qg = reinterpret_cast<const G *>(q + off);
+        const G *dg = reinterpret_cast<const G *>(dinv);
         double acc = 0.0, accz = 0.0;
         const T a_t = (T)alpha;
-        // Four independent elements per thread per pass: enough loads in
-        // flight for HBM speed with few CTAs per SM.
+        const TX a_x = (TX)alpha;
         const long long bd = blockDim.x;
-        long long i = beg + threadIdx.x;
-        for (; i + 3 * bd < end; i += 4 * bd) {
-            T pi[4], qi[4], ri[4];
-            TX xi[4];
+        auto one = [&](const G &pi, const G &qi, const G &ri0, const GX &xi0, long long gi) {
+            G rn;
+            GX xn;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                pi[u] = p[off + i + u * bd];
-                qi[u] = q[off + i + u * bd];
-                ri[u] = r[off + i + u * bd];
-                xi[u] = x[off + i + u * bd];
+            for (int k = 0; k < V; ++k) {
+                xn.v[k] = (TX)(xi0.v[k] + a_x * (TX)pi.v[k]);
+                rn.v[k] = ri0.v[k] - a_t * qi.v[k];
+                acc += (double)rn.v[k] * (double)rn.v[k];
             }
+            if (dinv) {
+                const G z = dg[gi];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                x[off + i + u * bd] = (TX)(xi[u] + (TX)alpha * (TX)pi[u]);
-                const T rn = ri[u] - a_t * qi[u];
-                r[off + i + u * bd] = rn;
-                acc += (double)rn * (double)rn;
-                if (dinv) accz += (double)dinv[i + u * bd] * (double)rn * (double)rn;
+                for (int k = 0; k < V; ++k) accz += (double)z.v[k] * (double)rn.v[k] * (double)rn.v[k];
             }
+            xg[gi] = xn;
+            rg[gi] = rn;
+        };
+        long long gi = gbeg + threadIdx.x;
+        for (; gi + bd < gend; gi += 2 * bd) {
+            const G p0 = pg[gi], p1 = pg[gi + bd];
+            const G q0 = qg[gi], q1 = qg[gi + bd];
+            const G r0 = rg[gi], r1 = rg[gi + bd];
+            const GX x0 = xg[gi], x1 = xg[gi + bd];
+            one(p0, q0, r0, x0, gi);
+            one(p1, q1, r1, x1, gi + bd);
         }
-        for (; i < end; i += bd) {
-            const T pi = p[off + i], qi = q[off + i];
-            x[off + i] = (TX)(x[off + i] + (TX)alpha * (TX)pi);
-            const T ri = r[off + i] - a_t * qi;
-            r[off + i] = ri;
-            acc += (double)ri * (double)ri;
-            if (dinv) accz += (double)dinv[i] * (double)ri * (double)ri;
-        }
+        if (gi < gend) one(pg[gi], qg[gi], rg[gi], xg[gi], gi);
         const double s = block_sum(acc, red);
         double sz = s;
         if (dinv) {
@@ -124,6 +144,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, const T *__restrict__ r, ColState st,
                                                          SolveParams sp, const int8_t *__restrict__ mask,
                                                          const T *__restrict__ dinv, int ncols) {
+    using G = Group<T>;
+    constexpr int V = G::N;
     const int nitems = ncols * sp.nchunks;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int col = item / sp.nchunks;
@@ -131,23 +153,35 @@ __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, cons
         if (st.status[col] != COL_ACTIVE) continue;
         if (mask && !mask[col]) continue;
         const T b = (T)st.beta[col];
-        const long long n = sp.colstride;
-        const long long beg = n * chunk / sp.nchunks, end = n * (chunk + 1) / sp.nchunks;
-        const long long off = (long long)col * n;
+        const long long ng = sp.colstride / V;
+        const long long gbeg = ng * chunk / sp.nchunks, gend = ng * (chunk + 1) / sp.nchunks;
+        const long long off = (long long)col * sp.colstride;
+        G *pg = reinterpret_cast<G *>(p + off);
+        const G *rg = reinterpret_cast<const G *>(r + off);
+        const G *dg = reinterpret_cast<const G *>(dinv);
         const long long bd = blockDim.x;
-        long long i = beg + threadIdx.x;
-        for (; i + 3 * bd < end; i += 4 * bd) {
-            T ri[4], pi[4], zi[4];
+        auto one = [&](const G &ri, const G &pi, long long gi) {
+            G pn;
+            if (dinv) {
+                const G z = dg[gi];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                ri[u] = r[off + i + u * bd];
-                pi[u] = p[off + i + u * bd];
-                zi[u] = dinv ? dinv[i + u * bd] : T(1);
+                for (int k = 0; k < V; ++k) pn.v[k] = z.v[k] * ri.v[k] + b * pi.v[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; ++k) pn.v[k] = ri.v[k] + b * pi.v[k];
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) p[off + i + u * bd] = (dinv ? zi[u] * ri[u] : ri[u]) + b * pi[u];
+            pg[gi] = pn;
+        };
+        long long gi = gbeg + threadIdx.x;
+        for (; gi + 3 * bd < gend; gi += 4 * bd) {
+            const G r0 = rg[gi], r1 = rg[gi + bd], r2 = rg[gi + 2 * bd], r3 = rg[gi + 3 * bd];
+            const G p0 = pg[gi], p1 = pg[gi + bd], p2 = pg[gi + 2 * bd], p3 = pg[gi + 3 * bd];
+            one(r0, p0, gi);
+            one(r1, p1, gi + bd);
+            one(r2, p2, gi + 2 * bd);
+            one(r3, p3, gi + 3 * bd);
         }
-        for (; i < end; i += bd) p[off + i] = (dinv ? dinv[i] * r[off + i] : r[off + i]) + b * p[off + i];
+        for (; gi < gend; gi += bd) one(rg[gi], pg[gi], gi);
     }
 }
 
