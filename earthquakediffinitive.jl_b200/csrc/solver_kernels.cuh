@@ -185,6 +185,221 @@ __global__ void __launch_bounds__(256) cg_pupdate_kernel(T *__restrict__ p, cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-staged versions of the two iteration vector kernels. The vectors of a
+// (column, chunk) item stream through shared memory in 4 KB tiles by bulk
+// copies (two stages, completing on mbarriers), so the bytes in flight cost
+// no registers: beside the other half's stencil CTAs an SM has about 8 K
+// registers and 110 KB of shared memory left, and these kernels use 32
+// registers a thread and 41 KB (update) or 25 KB (direction) a CTA. Same
+// per-element arithmetic as the register versions above (which the batch
+// setup and the FP64 iterations use); the partial sums of r.r are in a fixed
+// order.
+// ---------------------------------------------------------------------------
+constexpr int kVecStages = 2;
+constexpr int kVecTileBytes = 4096;
+constexpr size_t kUpdateBulkSmem = 64 + (size_t)kVecStages * 5 * kVecTileBytes;
+constexpr size_t kDirBulkSmem = 64 + (size_t)kVecStages * 3 * kVecTileBytes;
+
+// Tiles are counted over all items a CTA processes (`g`): tile g uses stage
+// g % kVecStages and completes that stage's mbarrier phase (g / kVecStages) & 1.
+__device__ __forceinline__ int vec_stage(unsigned g) { return (int)(g % kVecStages); }
+__device__ __forceinline__ unsigned vec_parity(unsigned g) { return (g / kVecStages) & 1u; }
+
+// After a bounded wait on tile g gave up (recorded in *err): wait (bounded)
+// once more for tile g and for tile g + 1 if it was issued, so that no copy
+// lands in shared memory after the CTA has left.
+__device__ __forceinline__ void vec_bulk_drain(uint64_t *bar, unsigned g, bool next_issued, unsigned *err) {
+    if (threadIdx.x == 0) {
+        mbar_wait_bounded(&bar[vec_stage(g)], vec_parity(g), err);
+        if (next_issued) mbar_wait_bounded(&bar[vec_stage(g + 1)], vec_parity(g + 1), err);
+    }
+    __syncthreads();
+}
+
+template <typename T, typename TX>
+__global__ void __launch_bounds__(128, 16) cg_update_bulk_kernel(
+    TX *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ q,
+    const double *__restrict__ apply_part, ColState st, SolveParams sp, double *__restrict__ rr_part,
+    const T *__restrict__ dinv, int ncols, unsigned *__restrict__ err) {
+    static_assert(sizeof(T) == sizeof(TX), "x and r share the group layout");
+    using G = Group<T>;
+    using GX = Group<TX>;
+    constexpr int V = G::N;
+    constexpr int TE = kVecTileBytes / (int)sizeof(T);  // elements per vector tile
+    constexpr int TG = TE / V;                          // groups per vector tile
+    extern __shared__ __align__(128) unsigned char vsm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(vsm);
+    T *buf = reinterpret_cast<T *>(vsm + 64);  // [stage][p, q, r, x, dinv][TE]
+    __shared__ double red[32];
+    __shared__ double s_alpha;
+    const unsigned nv = dinv ? 5u : 4u;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kVecStages; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g0 = 0;  // tiles this CTA started before the current item
+    const int nitems = ncols * sp.nchunks;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int col = item / sp.nchunks;
+        const int chunk = item % sp.nchunks;
+        if (st.status[col] != COL_ACTIVE) continue;
+        if (threadIdx.x == 0) {
+            double pq = 0.0, pp = 0.0;
+            for (int t = 0; t < sp.ntiles; ++t) {
+                pq += apply_part[((long long)col * sp.ntiles + t) * 2 + 0];
+                pp += apply_part[((long long)col * sp.ntiles + t) * 2 + 1];
+            }
+            double a = st.gamma[col] / pq;
+            if (!(pq > 2.220446049250313e-16 * pp) || !isfinite(a)) a = 0.0;  // breakdown: scalar kernel flags it
+            s_alpha = a;
+        }
+        __syncthreads();
+        const double alpha = s_alpha;
+        const long long ng = sp.colstride / V;
+        const long long e0 = ng * chunk / sp.nchunks * V, e1 = ng * (chunk + 1) / sp.nchunks * V;
+        const long long off = (long long)col * sp.colstride;
+        const int ntile = (int)((e1 - e0 + TE - 1) / TE);
+        auto issue = [&](int t) {
+            const int s = vec_stage(g0 + t);
+            const long long b0 = e0 + (long long)t * TE;
+            const unsigned bytes = (unsigned)(min((long long)TE, e1 - b0) * (long long)sizeof(T));
+            T *dst = buf + (size_t)s * 5 * TE;
+            mbar_arrive_expect_tx(&bar[s], nv * bytes);
+            bulk_g2s(dst + 0 * TE, p + off + b0, bytes, &bar[s]);
+            bulk_g2s(dst + 1 * TE, q + off + b0, bytes, &bar[s]);
+            bulk_g2s(dst + 2 * TE, r + off + b0, bytes, &bar[s]);
+            bulk_g2s(dst + 3 * TE, x + off + b0, bytes, &bar[s]);
+            if (dinv) bulk_g2s(dst + 4 * TE, dinv + b0, bytes, &bar[s]);
+        };
+        if (threadIdx.x == 0)
+            for (int t = 0; t < min(kVecStages, ntile); ++t) issue(t);
+        double acc = 0.0, accz = 0.0;
+        const T a_t = (T)alpha;
+        const TX a_x = (TX)alpha;
+        for (int t = 0; t < ntile; ++t) {
+            const int s = vec_stage(g0 + t);
+            const bool landed = mbar_wait_bounded(&bar[s], vec_parity(g0 + t), err);
+            if (!__syncthreads_and(landed)) {
+                vec_bulk_drain(bar, g0 + t, t + 1 < ntile, err);
+                return;
+            }
+            const long long b0 = e0 + (long long)t * TE;
+            const int ngrp = (int)(min((long long)TE, e1 - b0) / V);
+            const G *tile = reinterpret_cast<const G *>(buf + (size_t)s * 5 * TE);
+            GX *xg = reinterpret_cast<GX *>(x + off + b0);
+            G *rg = reinterpret_cast<G *>(r + off + b0);
+            for (int gi = threadIdx.x; gi < ngrp; gi += blockDim.x) {
+                const G pi = tile[gi], qi = tile[TG + gi], ri = tile[2 * TG + gi];
+                const GX xi = reinterpret_cast<const GX *>(tile)[3 * TG + gi];
+                G rn;
+                GX xn;
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    xn.v[k] = (TX)(xi.v[k] + a_x * (TX)pi.v[k]);
+                    rn.v[k] = ri.v[k] - a_t * qi.v[k];
+                    acc += (double)rn.v[k] * (double)rn.v[k];
+                }
+                if (dinv) {
+                    const G z = tile[4 * TG + gi];
+#pragma unroll
+                    for (int k = 0; k < V; ++k) accz += (double)z.v[k] * (double)rn.v[k] * (double)rn.v[k];
+                }
+                xg[gi] = xn;
+                rg[gi] = rn;
+            }
+            __syncthreads();  // stage s is read: refill it
+            if (threadIdx.x == 0 && t + kVecStages < ntile) issue(t + kVecStages);
+        }
+        g0 += (unsigned)ntile;
+        const double sum = block_sum(acc, red);
+        double sz = sum;
+        if (dinv) {
+            __syncthreads();
+            sz = block_sum(accz, red);
+        }
+        if (threadIdx.x == 0) {
+            rr_part[((long long)col * sp.nchunks + chunk) * 2 + 0] = sum;
+            rr_part[((long long)col * sp.nchunks + chunk) * 2 + 1] = sz;
+        }
+        __syncthreads();
+    }
+}
+
+// p = r + beta p (with a preconditioner: p = dinv r + beta p), bulk-staged.
+template <typename T>
+__global__ void __launch_bounds__(128, 16) cg_pupdate_bulk_kernel(T *__restrict__ p, const T *__restrict__ r,
+                                                                  ColState st, SolveParams sp,
+                                                                  const T *__restrict__ dinv, int ncols,
+                                                                  unsigned *__restrict__ err) {
+    using G = Group<T>;
+    constexpr int V = G::N;
+    constexpr int TE = kVecTileBytes / (int)sizeof(T);
+    constexpr int TG = TE / V;
+    extern __shared__ __align__(128) unsigned char vsm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(vsm);
+    T *buf = reinterpret_cast<T *>(vsm + 64);  // [stage][r, p, dinv][TE]
+    const unsigned nv = dinv ? 3u : 2u;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kVecStages; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g0 = 0;  // tiles this CTA started before the current item
+    const int nitems = ncols * sp.nchunks;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int col = item / sp.nchunks;
+        const int chunk = item % sp.nchunks;
+        if (st.status[col] != COL_ACTIVE) continue;
+        const T b = (T)st.beta[col];
+        const long long ng = sp.colstride / V;
+        const long long e0 = ng * chunk / sp.nchunks * V, e1 = ng * (chunk + 1) / sp.nchunks * V;
+        const long long off = (long long)col * sp.colstride;
+        const int ntile = (int)((e1 - e0 + TE - 1) / TE);
+        auto issue = [&](int t) {
+            const int s = vec_stage(g0 + t);
+            const long long b0 = e0 + (long long)t * TE;
+            const unsigned bytes = (unsigned)(min((long long)TE, e1 - b0) * (long long)sizeof(T));
+            T *dst = buf + (size_t)s * 3 * TE;
+            mbar_arrive_expect_tx(&bar[s], nv * bytes);
+            bulk_g2s(dst + 0 * TE, r + off + b0, bytes, &bar[s]);
+            bulk_g2s(dst + 1 * TE, p + off + b0, bytes, &bar[s]);
+            if (dinv) bulk_g2s(dst + 2 * TE, dinv + b0, bytes, &bar[s]);
+        };
+        if (threadIdx.x == 0)
+            for (int t = 0; t < min(kVecStages, ntile); ++t) issue(t);
+        for (int t = 0; t < ntile; ++t) {
+            const int s = vec_stage(g0 + t);
+            const bool landed = mbar_wait_bounded(&bar[s], vec_parity(g0 + t), err);
+            if (!__syncthreads_and(landed)) {
+                vec_bulk_drain(bar, g0 + t, t + 1 < ntile, err);
+                return;
+            }
+            const long long b0 = e0 + (long long)t * TE;
+            const int ngrp = (int)(min((long long)TE, e1 - b0) / V);
+            const G *tile = reinterpret_cast<const G *>(buf + (size_t)s * 3 * TE);
+            G *pg = reinterpret_cast<G *>(p + off + b0);
+            for (int gi = threadIdx.x; gi < ngrp; gi += blockDim.x) {
+                const G ri = tile[gi], pi = tile[TG + gi];
+                G pn;
+                if (dinv) {
+                    const G z = tile[2 * TG + gi];
+#pragma unroll
+                    for (int k = 0; k < V; ++k) pn.v[k] = z.v[k] * ri.v[k] + b * pi.v[k];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < V; ++k) pn.v[k] = ri.v[k] + b * pi.v[k];
+                }
+                pg[gi] = pn;
+            }
+            __syncthreads();  // stage s is read: refill it
+            if (threadIdx.x == 0 && t + kVecStages < ntile) issue(t + kVecStages);
+        }
+        g0 += (unsigned)ntile;
+    }
+}
+
 // Mixed precision: fold the FP32 correction into the FP64 solution.
 __global__ void __launch_bounds__(256) fold_correction_kernel(double *__restrict__ x, float *__restrict__ d, ColState st,
                                                               SolveParams sp, int ncols) {
