@@ -1326,6 +1326,28 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
     PinnedArr<double> &kstage = R.W->kstage;
     if (!generic && B.kcols && !B.kdev && kstage.n < 2 * gc.nf * chunk)
         CUDA_OR_RETURN(kstage.assign(2 * gc.nf * chunk, 0.0));
+    // Host K output: finished columns are staged in pinned memory, and the
+    // host copies them to the caller's K after the next graph launch, while
+    // the GPU runs those iterations.
+    const bool host_k = !generic && B.kcols && !B.kdev;
+    cudaEvent_t kready = nullptr;  // the staged columns have landed
+    if (host_k) CUDA_OR_RETURN(cudaEventCreateWithFlags(&kready, cudaEventDisableTiming));
+    struct EventGuard {
+        cudaEvent_t e;
+        ~EventGuard() {
+            if (e) cudaEventDestroy(e);
+        }
+    } kready_guard{kready};
+    std::vector<ColDone> staged;
+    auto copy_staged = [&]() -> int {
+        if (staged.empty()) return EQD_OK;
+        CUDA_OR_RETURN(cudaEventSynchronize(kready));
+        for (size_t j = 0; j < staged.size(); ++j)
+            std::memcpy(B.kcols + (size_t)staged[j].tag * 2 * gc.nf, kstage.data() + j * 2 * gc.nf,
+                        sizeof(double) * 2 * gc.nf);
+        staged.clear();
+        return EQD_OK;
+    };
     CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
     int next = 0, finished = 0;
     std::vector<ColDone> done;
@@ -1338,7 +1360,9 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
             if (rc) return rc;
             next += taken;
         }
-        rc = R.advance(done);
+        rc = R.launch();
+        if (!rc) rc = copy_staged();
+        if (!rc) rc = R.collect(done);
         if (rc) return rc;
         if (done.empty()) continue;
         if (!generic) {
@@ -1346,9 +1370,12 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
                 rc = R.extract(done, B.kdev, 2LL * gc.nf, true);
             } else {
                 rc = R.extract(done, R.W->kout.template as<double>(), 2LL * gc.nf, false);
-                if (!rc && B.kcols)
+                if (!rc && B.kcols) {
                     CUDA_OR_RETURN(cudaMemcpyAsync(kstage.data(), R.W->kout.p, sizeof(double) * 2 * gc.nf * done.size(),
                                                    cudaMemcpyDeviceToHost, G->stream));
+                    CUDA_OR_RETURN(cudaEventRecord(kready, G->stream));
+                    staged = done;
+                }
             }
             if (rc) return rc;
         } else if (B.u_out) {
@@ -1356,13 +1383,10 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
                 rc = R.solution(d.slot, B.u_out + (size_t)d.tag * ntot);
                 if (rc) return rc;
             }
+            CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
         }
-        CUDA_OR_RETURN(cudaStreamSynchronize(G->stream));
         for (size_t j = 0; j < done.size(); ++j) {
             const ColDone &d = done[j];
-            if (!generic && B.kcols && !B.kdev)
-                std::memcpy(B.kcols + (size_t)d.tag * 2 * gc.nf, kstage.data() + j * 2 * gc.nf,
-                            sizeof(double) * 2 * gc.nf);
             tot_it += d.iters;
             max_it = std::max<int64_t>(max_it, d.iters);
             if (d.status != COL_CONVERGED) ++unconv;
@@ -1373,6 +1397,8 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
         rc = R.release(done);
         if (rc) return rc;
     }
+    rc = copy_staged();
+    if (rc) return rc;
     CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
     CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
     float ms = 0.f;
