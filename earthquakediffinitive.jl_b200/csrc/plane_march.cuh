@@ -28,7 +28,8 @@
 // F_3 = lam G_3 + (lam+mu)(G_1+G_2), H21 = D1_2 v_1, H23 = D1_2 v_3 and
 // W_2 = D1_2 D1_2 (the wide operator, as a 1D matrix).
 //
-// Work decomposition (one CTA per (column, x2-tile)):
+// Work decomposition (one CTA per (column, x2 tile); FP64-input launches of
+// small batches also split the x3 march into segments, one CTA each):
 //   * one thread per point of the tile: both sides x all n1 points x the
 //     tile's x2 rows, grouped into warp-uniform classes (x2-interior rows,
 //     x2-closure rows, fault nodes with the two sides in adjacent lanes);
