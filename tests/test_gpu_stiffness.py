@@ -185,14 +185,16 @@ def test_x3_segmented_equals_whole_columns(eqd, precision):
         assert np.array_equal(K1[:, 0], Kb[:, c]) and it1[0] == itb[c]
 
 
-@pytest.mark.parametrize("dz, L_normal, l_f", [(100.0, 800.0, 400.0), (40.0, 800.0, 200.0)])
-def test_x3_segmented_bp8_grids(eqd, dz, L_normal, l_f):
+@pytest.mark.parametrize("dz, L_fault, L_normal, l_f", [(100.0, 800.0, 800.0, 400.0), (40.0, 800.0, 800.0, 200.0),
+                                                       (25.0, 200.0, 800.0, 100.0)])
+def test_x3_segmented_bp8_grids(eqd, dz, L_fault, L_normal, l_f):
     """The x3 split on the BP8 grids' n1-specialised FP64 instances (n1 = 9:
     17 x 17 x 9, one x2 tile, 162 columns; n1 = 21: 41 x 41 x 21, five x2
-    tiles, 242 columns): single columns (3 or 6 segments) give the same bits
+    tiles, 242 columns; n1 = 33: 17 x 17 x 33, three edge-partitioned x2
+    tiles, 162 columns): single columns (3 or 6 segments) give the same bits
     as the batch (2 segments, or none)."""
     mu = 32.04e9
-    fe = eqd.FaultElasticity(eqd.bp8_grids(dz, 800.0, L_normal), eqd.lame_lambda(mu, 0.25), mu, l_f,
+    fe = eqd.FaultElasticity(eqd.bp8_grids(dz, L_fault, L_normal), eqd.lame_lambda(mu, 0.25), mu, l_f,
                              precision="fp64")
     cols = np.arange(2 * fe.nf)
     Kb, itb, stb = eqd.stiffness_columns(fe, cols)
