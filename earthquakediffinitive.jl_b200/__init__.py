@@ -121,7 +121,14 @@ class CGSolver:
     (a FaultElasticity attaches its own). `precision` selects the engine:
     "fp64" is plain FP64 CG with Krylov.jl's stopping rule (recursive
     residual); "mixed" is FP32 CG with FP64 reliable updates, stopping on the
-    FP64 true residual."""
+    FP64 true residual. `chunk` caps the columns resident at once (0: as many
+    as `hbm_budget_bytes` allows), `reliable_delta` is the mixed engine's
+    residual-drop factor for an FP64 true-residual update, `tile_rows` pins
+    the stencil's x2 tile height (0: autotuned). `split` and `fuse` change
+    only the schedule, never the result bits: `split=False` runs a large
+    batch as one chain of kernels instead of two overlapping halves, and
+    `fuse=True` forms the CG direction inside the stencil apply (slower on
+    B200; for comparison)."""
 
     def __init__(self, fe=None, rtol=1e-10, atol=0.0, itmax=0, precond="none", precision="mixed",
                  chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0, split=True, fuse=False):
