@@ -123,8 +123,9 @@ class CGSolver:
     residual); "mixed" is FP32 CG with FP64 reliable updates, stopping on the
     FP64 true residual. `chunk` caps the columns resident at once (0: as many
     as `hbm_budget_bytes` allows), `reliable_delta` is the mixed engine's
-    residual-drop factor for an FP64 true-residual update, `tile_rows` pins
-    the stencil's x2 tile height (0: autotuned). `split` and `fuse` change
+    residual-drop factor for an FP64 true-residual update; `tile_rows` is
+    accepted and ignored (the stencil's launch variant belongs to the grid:
+    `autotune`, `set_stencil_variant`). `split` and `fuse` change
     only the schedule, never the result bits: `split=False` runs a large
     batch as one chain of kernels instead of two overlapping halves, and
     `fuse=True` forms the CG direction inside the stencil apply (slower on

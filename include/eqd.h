@@ -97,7 +97,9 @@ typedef struct {
     int32_t chunk;            /* columns per device batch; 0 -> as many as the HBM budget allows */
     double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.01) */
     uint64_t hbm_budget_bytes;/* 0 -> free device memory minus 2 GiB */
-    int32_t tile_rows;        /* x2 rows per CTA tile in the stencil; 0 -> autotuned */
+    int32_t tile_rows;        /* reserved, ignored: the stencil's launch variant (and with it the x2
+                                 tile height) belongs to the grid, chosen by eqd_autotune on first
+                                 use or fixed by eqd_set_variant */
     uint32_t flags;
 } eqd_solve_opts;
 
