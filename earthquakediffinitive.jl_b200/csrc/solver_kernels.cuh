@@ -200,6 +200,10 @@ constexpr int kVecStages = 2;
 constexpr int kVecTileBytes = 4096;
 constexpr size_t kUpdateBulkSmem = 64 + (size_t)kVecStages * 5 * kVecTileBytes;
 constexpr size_t kDirBulkSmem = 64 + (size_t)kVecStages * 3 * kVecTileBytes;
+// Launched without a shared-memory opt-in: dynamic plus the update kernel's
+// static 264 bytes must stay within the default 48 KB.
+static_assert(kUpdateBulkSmem + 264 <= 48 * 1024 && kDirBulkSmem <= 48 * 1024, "bulk vector tiles exceed 48 KB");
+static_assert(kVecTileBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // Tiles are counted over all items a CTA processes (`g`): tile g uses stage
 // g % kVecStages and completes that stage's mbarrier phase (g / kVecStages) & 1.
