@@ -1696,6 +1696,16 @@ extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_k
     return EQD_OK;
 }
 
+// The GEMV's first pass: 16-byte loads of K where K and n allow them
+// (gemv_vec2_ok), 8-byte loads otherwise.
+static void launch_gemv_partial(dim3 grid, cudaStream_t st, const double *K, const double *s, long long n, int nslice,
+                                int nvec, double *part) {
+    if (gemv_vec2_ok(K, n))
+        gemv_partial_kernel<true><<<grid, 256, 0, st>>>(K, s, n, nslice, nvec, part);
+    else
+        gemv_partial_kernel<false><<<grid, 256, 0, st>>>(K, s, n, nslice, nvec, part);
+}
+
 static int gemv_slices(int n) {
     // Enough CTAs to cover every SM several times over.
     const int rows_blocks = (n / 2 + 255) / 256;
@@ -1713,8 +1723,7 @@ extern "C" int eqd_kmat_gemv(eqd_kmat *M, const double *s, double *y, int32_t nv
     CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)n * nvec * nslice));
     CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, sizeof(double) * (size_t)n * nvec, cudaMemcpyHostToDevice, M->stream));
     dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
-    gemv_partial_kernel<<<grid, 256, 0, M->stream>>>(M->K.as<double>(), M->s.as<double>(), n, nslice, nvec,
-                                                     M->part.as<double>());
+    launch_gemv_partial(grid, M->stream, M->K.as<double>(), M->s.as<double>(), n, nslice, nvec, M->part.as<double>());
     const long long ne = (long long)n * nvec;
     gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, M->stream>>>(M->part.as<double>(), n, nslice, nvec,
                                                                            M->y.as<double>());
@@ -1791,7 +1800,7 @@ extern "C" int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_d
     nslice = std::max(1, std::min<int>(nslice, (int)(EQD_GEMV_STATIC_SCRATCH_DOUBLES / ((long long)n * nvec))));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
-    gemv_partial_kernel<<<grid, 256, 0, st>>>(K_device, s_device, n, nslice, nvec, scratch);
+    launch_gemv_partial(grid, st, K_device, s_device, n, nslice, nvec, scratch);
     const long long ne = (long long)n * nvec;
     gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(scratch, n, nslice, nvec, y_device);
     cudaError_t e = cudaGetLastError();
@@ -2267,8 +2276,7 @@ extern "C" int eqd_rhs_eval(eqd_rhs *R, double t, const double *u, double *du) {
     CUDA_OR_RETURN(cudaMemcpyAsync(R->u.p, u, sizeof(double) * nu, cudaMemcpyHostToDevice, st));
     CUDA_OR_RETURN(cudaMemsetAsync(R->status.p, 0, sizeof(unsigned), st));
     dim3 g1((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)R->nslice);
-    gemv_partial_kernel<<<g1, 256, 0, st>>>(R->K.as<double>(), R->u.as<double>(), n, R->nslice, 1,
-                                            R->part.as<double>());
+    launch_gemv_partial(g1, st, R->K.as<double>(), R->u.as<double>(), n, R->nslice, 1, R->part.as<double>());
     RhsParams P{};
     P.fr = friction_const(R->p);
     P.sigma0 = R->p.sigma0;

@@ -766,7 +766,22 @@ __global__ void toeplitz_expand_kernel(const double *__restrict__ src_cols, cons
 // go four at a time, so one pass over K serves four right-hand sides (the
 // time loop's Runge-Kutta stages or an ensemble): K is read ceil(nvec / 4)
 // times instead of nvec times.
+// VEC2: each thread reads its two rows of a column as one 16-byte load, which
+// needs K 16-byte aligned and n even (then every column starts on a 16-byte
+// boundary); gemv_vec2_ok() decides. Otherwise the two rows are read as two
+// 8-byte loads. Both forms add the same products in the same order.
 // ---------------------------------------------------------------------------
+__host__ __device__ inline bool gemv_vec2_ok(const void *K, long long n) {
+    return (n % 2 == 0) && ((reinterpret_cast<uintptr_t>(K) & 15u) == 0);
+}
+
+template <bool VEC2>
+__device__ __forceinline__ double2 gemv_load2(const double *__restrict__ K, long long off) {
+    if constexpr (VEC2) return *reinterpret_cast<const double2 *>(K + off);
+    else return make_double2(K[off], K[off + 1]);
+}
+
+template <bool VEC2>
 __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restrict__ K, const double *__restrict__ s,
                                                            long long n, int nslice, int nvec,
                                                            double *__restrict__ part) {
@@ -787,7 +802,7 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
             for (; c + 4 <= c1; c += 4) {  // four columns in flight per thread
                 double2 kk[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) kk[j] = *reinterpret_cast<const double2 *>(K + (c + j) * n + row2);
+                for (int j = 0; j < 4; ++j) kk[j] = gemv_load2<VEC2>(K, (c + j) * n + row2);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
 #pragma unroll
@@ -801,7 +816,7 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
                 }
             }
             for (; c < c1; ++c) {
-                const double2 kk = *reinterpret_cast<const double2 *>(K + c * n + row2);
+                const double2 kk = gemv_load2<VEC2>(K, c * n + row2);
 #pragma unroll
                 for (int u = 0; u < VB; ++u) {
                     if (u < nv) {

@@ -4,7 +4,7 @@
  * Drop-in for the dense fault-stiffness path of EarthquakeDiffinitive.jl:
  * one CG solve per unit-slip right-hand side on the split-node SBP-SAT
  * elastic operator A = -H P (D + SAT) P, assembled into K : [s2; s3] -> [dtau2; dtau3].
- * The Julia side binds these with `ccall` (see INTEGRATION.md). All buffers in
+ * The Julia side binds these with `ccall`. All buffers in
  * the signatures are HOST memory owned by the caller; the library owns its
  * device memory. Matrices are column-major FP64, exactly the layout of the
  * reference's `Matrix{Float64}`.
@@ -200,7 +200,8 @@ int eqd_set_variant(eqd_grid *grid, int32_t variant);
 int eqd_diag(eqd_grid *grid, double *d);
 
 /* Time-loop GEMV `mul!(Δτ, K, slip)` (src/BP8.jl:366) ----------------------
- * K stays resident on the device; y = K s for nvec vectors (n x nvec each). */
+ * K stays resident on the device; y = K s for nvec vectors (n x nvec each),
+ * any n >= 1. */
 int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out);
 int eqd_kmat_gemv(eqd_kmat *kmat, const double *s, double *y, int32_t nvec);
 int eqd_kmat_destroy(eqd_kmat *kmat);
@@ -208,12 +209,16 @@ int eqd_kmat_destroy(eqd_kmat *kmat);
 /* Allocation-free y = K s (no counterpart in the reference: an addition for
  * callers that cannot allocate device memory, e.g. a time loop inside CUDA
  * graph capture or under a framework's own allocator). K (n x n, column-major),
- * s and y (n x nvec) are DEVICE pointers owned by the caller, on `device`.
- * Scratch is a static 4 MiB array per device: n * nvec must not exceed
- * 524,288 (EQD_ERR_ARG otherwise). The first call on a device looks the array
- * up (make it before any stream capture). Launches on `stream` (a
- * cudaStream_t, NULL = default stream) and returns without synchronizing;
- * calls that overlap on the GPU share the scratch and race. */
+ * s and y (n x nvec) are DEVICE pointers owned by the caller, on `device`;
+ * any n >= 1 and any 8-byte-aligned K (16-byte loads are used only when K is
+ * 16-byte aligned and n is even). Scratch is a static 4 MiB array per device:
+ * n * nvec must not exceed 524,288 (EQD_ERR_ARG otherwise). The first call on
+ * a device looks the array's address up and caches it for the life of the
+ * process (make that call before any stream capture; the cached address does
+ * not survive a reset of the device's primary context, e.g. cudaDeviceReset).
+ * Launches on `stream` (a cudaStream_t, NULL = default stream) and returns
+ * without synchronizing. All calls on a device share the scratch array:
+ * serialise them (one stream, or events); calls that overlap on the GPU race. */
 int eqd_kmat_gemv_static(int32_t device, int32_t n, const double *K_device, const double *s_device,
                          double *y_device, int32_t nvec, void *stream);
 
