@@ -123,16 +123,17 @@ class CGSolver:
     residual); "mixed" is FP32 CG with FP64 reliable updates, stopping on the
     FP64 true residual. `chunk` caps the columns resident at once (0: as many
     as `hbm_budget_bytes` allows), `reliable_delta` is the mixed engine's
-    residual-drop factor for an FP64 true-residual update; `tile_rows` is
-    accepted and ignored (the stencil's launch variant belongs to the grid:
-    `autotune`, `set_stencil_variant`). `split` and `fuse` change
+    residual-drop factor for an FP64 true-residual update; `variant` picks
+    the FP32 stencil launch variant for this solver's calls (0: the grid's,
+    chosen by `autotune` on first use or pinned by `set_stencil_variant`;
+    k > 0: variant k - 1 of `autotune`'s list). `split` and `fuse` change
     only the schedule, never the result bits: `split=False` runs a large
     batch as one chain of kernels instead of two overlapping halves, and
     `fuse=True` forms the CG direction inside the stencil apply (slower on
     B200; for comparison)."""
 
     def __init__(self, fe=None, rtol=1e-10, atol=0.0, itmax=0, precond="none", precision="mixed",
-                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, tile_rows=0, split=True, fuse=False):
+                 chunk=0, reliable_delta=0.01, hbm_budget_bytes=0, variant=0, split=True, fuse=False):
         if precond not in _PRECONDS:
             raise EqdArgumentError(_abi.EQD_ERR_ARG, f"precond must be :none or :jacobi, got {precond}")
         if precision not in _PRECISIONS:
@@ -141,7 +142,7 @@ class CGSolver:
         self.rtol, self.atol, self.itmax = float(rtol), float(atol), int(itmax)
         self.precond, self.precision = precond, precision
         self.chunk, self.reliable_delta = int(chunk), float(reliable_delta)
-        self.hbm_budget_bytes, self.tile_rows = int(hbm_budget_bytes), int(tile_rows)
+        self.hbm_budget_bytes, self.variant = int(hbm_budget_bytes), int(variant)
         self.split = bool(split)
         self.fuse = bool(fuse)
         self.stats = CGStats()
@@ -155,7 +156,7 @@ class CGSolver:
         o.chunk = self.chunk
         o.reliable_delta = self.reliable_delta
         o.hbm_budget_bytes = self.hbm_budget_bytes
-        o.tile_rows = self.tile_rows
+        o.variant = self.variant
         if not self.split:
             o.flags |= _abi.EQD_FLAG_NO_SPLIT
         if self.fuse:
@@ -175,7 +176,7 @@ class CGSolver:
     def duplicate(self):
         """`duplicate(solver)`: same operator and options, fresh counters."""
         return CGSolver(self.fe, self.rtol, self.atol, self.itmax, self.precond, self.precision,
-                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.tile_rows, self.split,
+                        self.chunk, self.reliable_delta, self.hbm_budget_bytes, self.variant, self.split,
                         self.fuse)
 
     def report(self):
@@ -258,7 +259,8 @@ def set_stencil_variant(fe, variant):
 
 
 def autotune(fe, ncols=256):
-    """Time every FP32 stencil launch variant; returns (selected, [(tile_rows, threads, ms)])."""
+    """Time every FP32 stencil launch variant; returns (selected, [(tile_rows, threads, ms)]),
+    the list indexed by variant (`set_stencil_variant`, CGSolver(variant=k + 1))."""
     sel, nv = C.c_int32(), C.c_int32()
     ms, tr, tt = (C.c_double * 16)(), (C.c_int32 * 16)(), (C.c_int32 * 16)()
     check(lib().eqd_autotune(fe.handle, C.c_int32(ncols), C.byref(sel), ms, tr, tt, C.byref(nv)))

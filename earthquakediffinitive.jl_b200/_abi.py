@@ -48,7 +48,7 @@ class SolveOpts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("itmax", C.c_int64),
                 ("precond", C.c_int32), ("precision", C.c_int32), ("chunk", C.c_int32),
                 ("reliable_delta", C.c_double), ("hbm_budget_bytes", C.c_uint64),
-                ("tile_rows", C.c_int32), ("flags", C.c_uint32)]
+                ("variant", C.c_int32), ("flags", C.c_uint32)]
 
 
 class Stats(C.Structure):

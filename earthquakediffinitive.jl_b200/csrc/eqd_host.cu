@@ -413,7 +413,7 @@ extern "C" void eqd_default_opts(eqd_solve_opts *o) {
     o->chunk = 0;
     o->reliable_delta = 0.01;
     o->hbm_budget_bytes = 0;
-    o->tile_rows = 0;
+    o->variant = 0;
     o->flags = 0;
 }
 
@@ -1427,11 +1427,24 @@ static int run_batch_any(eqd_grid *G, const eqd_solve_opts *opts, const BatchSpe
         return fail(EQD_ERR_ARG, "precond must be :none or :jacobi");
     if (o.precision != EQD_PREC_FP64 && o.precision != EQD_PREC_MIXED) return fail(EQD_ERR_ARG, "unknown precision");
     if (B.rhs && o.precision != EQD_PREC_FP64) return fail(EQD_ERR_UNSUPPORTED, "explicit-RHS solves run in FP64");
+    if (o.variant < 0 || o.variant > kNumVariants)
+        return fail(EQD_ERR_ARG, "variant must be 0 (the grid's) or 1.." + std::to_string(kNumVariants));
     const auto t0 = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(G->mtx);
     if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    // A per-call variant replaces the grid's selection for this call only.
+    const int sel_before = G->sel32;
+    const bool tuned_before = G->tuned;
+    if (o.variant > 0) {
+        G->sel32 = o.variant - 1;
+        G->tuned = true;
+    }
     int rc = o.precision == EQD_PREC_MIXED ? run_batch<float>(G, o, B, stats) : run_batch<double>(G, o, B, stats);
+    if (o.variant > 0) {
+        G->sel32 = sel_before;
+        G->tuned = tuned_before;
+    }
     if (stats)
         stats->seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;
@@ -1625,14 +1638,16 @@ extern "C" int eqd_profile_apply(eqd_grid *G, int32_t ncols, int32_t precision, 
 
 extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, double *ms_per_variant,
                             int32_t *tile_rows, int32_t *threads, int32_t *nvariants) {
-    if (!G || ncols < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    if (!G || ncols < 0) return fail(EQD_ERR_ARG, "invalid argument");
     std::lock_guard<std::mutex> lk(G->mtx);
     if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
-    eqd_solve_opts o;
-    eqd_default_opts(&o);
-    int rc = tune_by_iterations(G, o, ncols);
-    if (rc) return rc;
+    if (ncols > 0) {
+        eqd_solve_opts o;
+        eqd_default_opts(&o);
+        int rc = tune_by_iterations(G, o, ncols);
+        if (rc) return rc;
+    }
     if (selected) *selected = G->sel32;
     if (nvariants) *nvariants = kNumVariants;
     for (int v = 0; v < kNumVariants; ++v) {

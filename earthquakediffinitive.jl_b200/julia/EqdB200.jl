@@ -35,7 +35,7 @@ mutable struct SolveOpts
     rtol::Float64; atol::Float64; itmax::Int64
     precond::Int32; precision::Int32; chunk::Int32
     reliable_delta::Float64; hbm_budget_bytes::UInt64
-    tile_rows::Int32; flags::UInt32
+    variant::Int32; flags::UInt32
 end
 
 mutable struct Stats
@@ -62,7 +62,7 @@ function default_opts(; rtol=1e-10, atol=0.0, itmax=0, precond=:none, precision=
 end
 
 """
-    GpuFaultElasticity(n1, n23, Δz, L_fault, L_normal, λ, μ; l_f, device=0, solver_kwargs...)
+    GpuFaultElasticity(n1, n23, L_fault, L_normal, λ, μ; l_f, device=0, solver_kwargs...)
 
 The device-side analogue of `FaultElasticity` for `build_model`'s grids
 (src/BP8.jl:196-206): minus block x1 ∈ [-L_normal, 0], plus block

@@ -97,9 +97,9 @@ typedef struct {
     int32_t chunk;            /* columns per device batch; 0 -> as many as the HBM budget allows */
     double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.01) */
     uint64_t hbm_budget_bytes;/* 0 -> free device memory minus 2 GiB */
-    int32_t tile_rows;        /* reserved, ignored: the stencil's launch variant (and with it the x2
-                                 tile height) belongs to the grid, chosen by eqd_autotune on first
-                                 use or fixed by eqd_set_variant */
+    int32_t variant;          /* FP32 stencil launch variant for this call: 0 -> the grid's (chosen by
+                                 eqd_autotune on first use, or pinned by eqd_set_variant); k > 0 ->
+                                 variant k - 1 of eqd_autotune's list, for this call only */
     uint32_t flags;
 } eqd_solve_opts;
 
@@ -188,7 +188,9 @@ int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t 
  * size, columns per thread, edge-partitioned tiles): times 20 mixed-precision
  * CG iterations of ncols unit-slip columns (<= 2nf) with every variant, keeps
  * the fastest for this grid (used by every later mixed-precision call) and
- * reports milliseconds per iteration. Arrays hold *nvariants (<= 16) entries. */
+ * reports milliseconds per iteration. Arrays hold *nvariants (<= 16) entries.
+ * ncols = 0 re-tunes nothing: it reports the current selection and the times
+ * of the last tuning (zeros if the grid was never tuned). */
 int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_per_variant, int32_t *tile_rows,
                  int32_t *threads, int32_t *nvariants);
 

@@ -1,6 +1,6 @@
 """Time the stencil apply (the CG iteration's kernel) on a BP8 grid.
 
-    python earthquakediffinitive.jl_b200/profile_apply.py --dz 50 --columns 512 [--variant 2]
+    python profile_apply.py --dz 50 --columns 512 [--variant 2]
 
 Grids follow `build_model` (src/BP8.jl:196-206): blocks of
 (L_normal/dz+1) x (2 L_fault/dz+1)^2 nodes per side, mu = 32.04 GPa, nu = 0.25.
@@ -15,7 +15,7 @@ import importlib.util
 import os
 import sys
 
-PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "earthquakediffinitive.jl_b200")
 
 
 def _package():
