@@ -16,7 +16,8 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libeqd.so")
 SOURCES = [os.path.join(CSRC, "eqd_host.cu")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in
-                  ("eqd_common.cuh", "plane_march.cuh", "solver_kernels.cuh", "rhs_kernels.cuh", "ops_tables.h")] + \
+                  ("eqd_common.cuh", "plane_march.cuh", "ring_march.cuh", "solver_kernels.cuh", "rhs_kernels.cuh",
+                   "ops_tables.h")] + \
     [os.path.join(HERE, "..", "include", "eqd.h")]
 
 NVCC_FLAGS = [

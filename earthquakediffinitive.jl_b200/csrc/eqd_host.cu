@@ -20,6 +20,7 @@
 #include "ops_tables.h"
 #include "solver_kernels.cuh"
 #include "rhs_kernels.cuh"
+#include "ring_march.cuh"
 
 using namespace eqd;
 
@@ -71,6 +72,8 @@ struct MarchCfg {
     int threads = 0;
     size_t smem = 0;
     size_t smem_af = 0;  // MODE_AF (second plane ring); 0: does not fit, the direction update runs apart
+    int ring_t2 = 0;     // > 0: the FP32 A-apply runs ring_march_kernel with this x2 tile capacity
+    RingGeom rg{};
 };
 
 static constexpr int kMaxT32 = 640;   // generic FP32 instances
@@ -78,7 +81,70 @@ static constexpr int kMaxT32b = 512;  // FP32 A-apply variant without register s
 static constexpr int kMaxT32c = 384;  // FP32 A-apply, two columns per thread
 static constexpr int kMaxT64 = 384;
 static constexpr int kMaxT64b = 512;  // FP64 instances for wide x1 lines (n1 = 33 needs 7 x 66 threads)
-static constexpr int kNumVariants = 9;
+static constexpr int kNumVariants = 11;  // 9 plane-march variants, then 2 ring-march variants
+static constexpr int kFirstRingVariant = 9;
+
+// Ring-march instances per n1: (x2 tile capacity, register cap per thread)
+// of its two variants. 136 registers hold a step without spills; a CTA's
+// threads x registers must stay within the SM's 65,536 (n1 = 33 takes fewer
+// registers and spills a little).
+template <int N1> struct RingTraits;
+template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 136, T2B = 14, MB = 136; };
+template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 136, T2B = 10, MB = 136; };
+template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 120, T2B = 8, MB = 104; };
+static_assert(ring_threads(9, RingTraits<9>::T2B) * RingTraits<9>::MB <= 65536, "ring CTA exceeds the register file");
+static_assert(ring_threads(21, RingTraits<21>::T2B) * RingTraits<21>::MB <= 65536, "ring CTA exceeds the register file");
+static_assert(ring_threads(33, RingTraits<33>::T2A) * RingTraits<33>::MA <= 65536, "ring CTA exceeds the register file");
+static_assert(ring_threads(33, RingTraits<33>::T2B) * RingTraits<33>::MB <= 65536, "ring CTA exceeds the register file");
+
+static int ring_t2_for(int n1, int which) {
+    switch (n1) {
+    case 9: return which == 0 ? RingTraits<9>::T2A : RingTraits<9>::T2B;
+    case 21: return which == 0 ? RingTraits<21>::T2A : RingTraits<21>::T2B;
+    case 33: return which == 0 ? RingTraits<33>::T2A : RingTraits<33>::T2B;
+    default: return 0;
+    }
+}
+
+// Launch configuration of ring_march_kernel: 7-row tiles at both x2 ends,
+// the rows between split into tiles of at most t2 rows.
+static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::string &why) {
+    if (t2 <= 0) {
+        why = "ring march: n1 = " + std::to_string(gc.n1) + " has no specialised instance";
+        return false;
+    }
+    if (gc.n2 < 2 * kRingEdge) {
+        why = "ring march: n2 below 14";
+        return false;
+    }
+    const int m = gc.n2 - 2 * kRingEdge;
+    const int nmid = m > 0 ? (m + t2 - 1) / t2 : 0;
+    out = MarchCfg{};
+    out.ring_t2 = t2;
+    out.rg.n2 = gc.n2;
+    out.rg.n3 = gc.n3;
+    out.rg.PS = gc.PS;
+    out.rg.colstride = gc.colstride;
+    out.rg.ntiles = nmid + 2;
+    out.rg.nmid = std::max(nmid, 1);
+    out.rg.drop_plane = -1;
+    out.rg.poll_limit = 0;
+    out.g.n1 = gc.n1;
+    out.g.n2 = gc.n2;
+    out.g.n3 = gc.n3;
+    out.g.PS = gc.PS;
+    out.g.colstride = gc.colstride;
+    out.g.ntiles = out.rg.ntiles;
+    out.g.t2max = t2;
+    out.g.nblk = 1;
+    out.g.nseg = 1;
+    out.g.segblk = 1;
+    out.g.edge = kRingEdge;
+    out.threads = ring_threads(gc.n1, t2);
+    out.smem = ring_smem(gc.n1, t2);
+    out.smem_af = 0;  // the direction update is not fused into this kernel
+    return true;
+}
 
 static bool n1_specialized(int n1) { return n1 == 9 || n1 == 21 || n1 == 33; }
 
@@ -272,6 +338,8 @@ struct eqd_grid {
     std::mutex mtx;
     std::vector<double> x2f, x3f;
     int tile_rows = 0;
+    int test_drop_plane = -1;      // eqd_test_inject_wait_timeout: the next ring launch never copies this plane
+    unsigned test_poll_limit = 0;
 };
 
 struct eqd_kmat {
@@ -305,6 +373,39 @@ static void launch_n1(int n1, dim3 grid, const MarchCfg &m, cudaStream_t st, con
     }
 }
 
+template <int N1>
+static void launch_ring_n1(int t2, dim3 grid, const MarchCfg &m, const RingGeom &rg, cudaStream_t st,
+                           const OpConst<float> &C, const float *in, float *out, const int8_t *status,
+                           double *partials, unsigned *err) {
+    using R = RingTraits<N1>;
+    if (t2 == R::T2A)
+        ring_march_kernel<N1, R::T2A, R::MA><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
+    else
+        ring_march_kernel<N1, R::T2B, R::MB><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
+}
+
+// The FP32 CG apply through ring_march_kernel (one CTA per column and x2
+// tile). A pending test injection (eqd_test_inject_wait_timeout) applies to
+// this launch only.
+static cudaError_t launch_ring(eqd_grid *G, const MarchCfg &m, const float *in, float *out, const ColumnSet &cs,
+                               double *partials, int ncols, cudaStream_t st) {
+    RingGeom rg = m.rg;
+    if (G->test_drop_plane >= 0) {
+        rg.drop_plane = G->test_drop_plane;
+        rg.poll_limit = G->test_poll_limit;
+        G->test_drop_plane = -1;
+    }
+    const dim3 grid((unsigned)((long long)ncols * rg.ntiles));
+    unsigned *err = G->err.as<unsigned>();
+    switch (G->gc.n1) {
+    case 9: launch_ring_n1<9>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    case 21: launch_ring_n1<21>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    case 33: launch_ring_n1<33>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template <typename T, typename TO, int MODE>
 static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs, double *partials, int ncols,
                                 int variant = -1, cudaStream_t stream = nullptr) {
@@ -313,6 +414,11 @@ static cudaError_t launch_march(eqd_grid *G, const T *in, TO *out, ColumnSet cs,
     const int n1 = G->gc.n1;
     if constexpr (sizeof(T) == 4 && (MODE == MODE_A || MODE == MODE_AF)) {
         const int v = variant >= 0 ? variant : G->sel32;
+        if (G->v32[v].ring_t2 > 0) {
+            if (MODE == MODE_AF) return cudaErrorInvalidValue;  // not fused in this kernel (smem_af = 0)
+            return launch_ring(G, G->v32[v], reinterpret_cast<const float *>(in), reinterpret_cast<float *>(out), cs,
+                               partials, ncols, st);
+        }
         const int lanes = G->v32_lanes[v];
         const long long groups = (ncols + lanes - 1) / lanes;
         MarchCfg m = segmented(G->v32[v], groups, G->num_sms);
@@ -371,12 +477,17 @@ static cudaError_t configure_kernels(int smem_max) {
         (const void *)plane_march_kernel<float, float, MODE_AF, kMaxT32c, N, 2>,         \
         (const void *)plane_march_kernel<double, double, MODE_AF, kMaxT64, N, 1>,        \
         (const void *)plane_march_kernel<double, double, MODE_AF, kMaxT64b, N, 1>,
+#define EQD_RING_KS(N)                                                                                     \
+    (const void *)ring_march_kernel<N, RingTraits<N>::T2A, RingTraits<N>::MA>,                             \
+        (const void *)ring_march_kernel<N, RingTraits<N>::T2B, RingTraits<N>::MB>,
     const void *ks[] = {
         EQD_FOR_N1(EQD_KS) EQD_KS(0)
         (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32, 0, 1>,
         (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64, 0, 1>,
         (const void *)plane_march_kernel<double, double, MODE_AP, kMaxT64b, 0, 1>,
+        EQD_FOR_N1(EQD_RING_KS)
     };
+#undef EQD_RING_KS
 #undef EQD_KS
     for (const void *k : ks) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
@@ -507,17 +618,26 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     {
         // thread limit, kernel launch bound, columns per thread, tile rows
         // (0: as many as fit), edge partition
-        const int lim[kNumVariants] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192, kMaxT32b, kMaxT32b, 192, 448};
-        const int mt[kNumVariants] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c, kMaxT32b, kMaxT32b,
-                                      kMaxT32b, kMaxT32b};
-        const int ln[kNumVariants] = {1, 1, 1, 2, 2, 1, 1, 1, 1};
-        const int rows[kNumVariants] = {0, 0, 0, 0, 0, 7, 10, 0, 0};
-        const bool edg[kNumVariants] = {false, false, false, false, false, true, true, false, false};
+        const int lim[kFirstRingVariant] = {kMaxT32, kMaxT32b, 256, kMaxT32c, 192, kMaxT32b, kMaxT32b, 192, 448};
+        const int mt[kFirstRingVariant] = {kMaxT32, kMaxT32b, kMaxT32b, kMaxT32c, kMaxT32c, kMaxT32b, kMaxT32b,
+                                           kMaxT32b, kMaxT32b};
+        const int ln[kFirstRingVariant] = {1, 1, 1, 2, 2, 1, 1, 1, 1};
+        const int rows[kFirstRingVariant] = {0, 0, 0, 0, 0, 7, 10, 0, 0};
+        const bool edg[kFirstRingVariant] = {false, false, false, false, false, true, true, false, false};
         for (int v = 0; v < kNumVariants; ++v) {
-            G->v32_maxt[v] = mt[v];
-            G->v32_lanes[v] = ln[v];
-            if (!make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], rows[v], gc, G->v32[v],
-                                       why, ln[v], mt[v], edg[v])) {
+            bool ok;
+            if (v < kFirstRingVariant) {
+                G->v32_maxt[v] = mt[v];
+                G->v32_lanes[v] = ln[v];
+                ok = make_march_cfg<float>(gc.n1, gc.n2, gc.n3, gc.PS, gc.colstride, lim[v], rows[v], gc, G->v32[v],
+                                           why, ln[v], mt[v], edg[v]);
+            } else {
+                // Ring-march variants: the BP8 lines (n1 = 9, 21, 33) only.
+                G->v32_maxt[v] = 0;
+                G->v32_lanes[v] = 1;
+                ok = make_ring_cfg(gc, ring_t2_for(gc.n1, v - kFirstRingVariant), G->v32[v], why);
+            }
+            if (!ok) {
                 G->v32[v] = G->m32;  // fall back to the generic configuration
                 G->v32_maxt[v] = kMaxT32;
                 G->v32_lanes[v] = 1;
@@ -1664,6 +1784,17 @@ extern "C" int eqd_set_variant(eqd_grid *G, int32_t variant) {
     if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
     G->sel32 = variant;
     G->tuned = true;
+    return EQD_OK;
+}
+
+extern "C" int eqd_test_inject_wait_timeout(eqd_grid *G, int32_t plane, uint32_t poll_limit) {
+    if (!G || plane < 0 || plane >= G->gc.n3 || poll_limit == 0) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
+    if (G->v32[G->sel32].ring_t2 <= 0)
+        return fail(EQD_ERR_UNSUPPORTED, "the grid's FP32 apply variant is not a ring-march variant");
+    G->test_drop_plane = plane;
+    G->test_poll_limit = poll_limit;
     return EQD_OK;
 }
 

@@ -198,6 +198,14 @@ int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_pe
  * for this grid instead of autotuning (reproducibility across processes). */
 int eqd_set_variant(eqd_grid *grid, int32_t variant);
 
+/* Failure-path test hook (no counterpart in the reference): the next FP32
+ * stencil apply of this grid (its selected variant must be a ring-march
+ * variant) never issues the copy of x3 plane `plane` and gives every bounded
+ * wait `poll_limit` polls. The waits on that plane give up, the kernel drains
+ * its other copies and returns, and the call that launched it returns
+ * EQD_ERR_TIMEOUT; later calls run normally. One launch only. */
+int eqd_test_inject_wait_timeout(eqd_grid *grid, int32_t plane, uint32_t poll_limit);
+
 /* Jacobi diagonal, `diag(A)` (src/ElasticitySplitNode.jl:352-357), reference layout. */
 int eqd_diag(eqd_grid *grid, double *d);
 
