@@ -71,7 +71,7 @@ def test_apply_columns_independent(eqd):
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}")
-@pytest.mark.parametrize("variant", list(range(9)))
+@pytest.mark.parametrize("variant", list(range(11)))
 def test_cg_path_kernel_every_variant(eqd, case, variant):
     """The kernel the CG iterations run (input already in range(P)), for each
     FP32 launch variant the autotuner may pick, and in FP64."""

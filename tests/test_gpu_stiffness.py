@@ -88,7 +88,7 @@ def test_batched_equals_single(eqd, precision):
     _batched_equals_single(eqd, precision, None)
 
 
-@pytest.mark.parametrize("variant", list(range(9)))
+@pytest.mark.parametrize("variant", list(range(11)))
 def test_batched_equals_single_every_variant(eqd, variant):
     """Bit-identity holds for every stencil launch variant, including the
     two-columns-per-thread ones (a column's partner lane must not matter)."""
