@@ -1,18 +1,21 @@
 """Benchmark of the fault-stiffness build on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config h50]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config h20]
 
-Workload (default `h50`): the BP8 grid at h = 50 m, L_fault = 800 m,
-L_normal = 400 m (33 x 33 x 9 nodes per side, 58,806 DOF), Omega_f = the whole
-fault plane (l_f = L_fault), i.e. all 2,178 unit-slip columns of K. One step =
-one build of those K columns by batched mixed-precision CG (FP32 stencil and
-vector updates, FP64 reliable updates, rtol 1e-10 on the FP64 true residual),
-traction extraction included. Inputs are unit slips (synthetic by
-definition; no dataset is involved).
+Workload (default `h20`): the BP8 grid at h = 20 m, L_fault = 800 m,
+L_normal = 400 m (81 x 81 x 21 nodes per side, 826,686 DOF), Omega_f = the
+whole fault plane (l_f = L_fault), i.e. all 13,122 unit-slip columns of K.
+One step = one build of those K columns by batched mixed-precision CG (FP32
+stencil and vector updates, FP64 reliable updates, rtol 1e-10 on the FP64
+true residual), traction extraction included; columns refill CG slots as
+others finish. Inputs are unit slips (synthetic by definition; no dataset is
+involved). `--config h50` runs the h = 50 m grid (2,178 columns).
 
 Prints one JSON line (rank 0). `value` = K columns/s with K written to
 device memory; `e2e` = the same through the public host API (`fault_stiffness`
-into a host array, every step). Under torchrun (N > 1) each rank builds a
+into a host array, every step). `serving` = per-request latency of a short
+seeded Poisson mix of column requests over the four BP8 grids answered by the
+continuous-batching server. Under torchrun (N > 1) each rank builds a
 contiguous shard of the columns on its own GPU (no collective on the data
 path); the step time is the max over ranks.
 """
@@ -65,8 +68,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="h50")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="h20")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=48, help="requests of the serving mix (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the serving mix (req/s)")
     return ap.parse_args()
 
 
@@ -188,6 +193,84 @@ def cpu_port_sample(cfg, ncols_sample, seed=0, threads=0):
     return ofe, ref, cols, nt
 
 
+def apply_kernel_name(variant, n1, tile_rows, threads):
+    """The FP32 CG apply kernel a launch variant runs: variants 9 and 10 are
+    the ring march on the lines it is built for (a CTA of 2 x roundup32(t2 n1)
+    + roundup32(2 t2) threads), every other variant the plane march."""
+    r32 = lambda x: (x + 31) // 32 * 32
+    if variant >= 9 and threads == 2 * r32(tile_rows * n1) + r32(2 * tile_rows):
+        return f"ring_march_kernel<n1={n1},t2={tile_rows}>"
+    return "plane_march_kernel<float,MODE_A>"
+
+
+def cpu_model():
+    """The host CPU's model name (first processor of /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+SERVE_GRIDS = {  # h: (dz, L_fault, L_normal, weight); Omega_f = the whole fault plane
+    100: (100.0, 800.0, 800.0, 0.4),
+    50: (50.0, 800.0, 400.0, 0.3),
+    25: (25.0, 1600.0, 800.0, 0.2),
+    20: (20.0, 800.0, 400.0, 0.1),
+}
+
+
+def serving_leg(eqd, device, nreq, rate, check=4, seed=5):
+    """The serving mix (Poisson arrivals at `rate` req/s; grid h in {100, 50,
+    25, 20} m with weights .4/.3/.2/.1; floor(exp(U(0, ln 512))) + 1 seeded
+    unit-slip columns per request; HBM budget 150 GB) through the
+    continuous-batching server. Latency = submit -> last K column delivered
+    to the request's host buffer, per request."""
+    from eqd_b200.serving import run_mix
+    lam = eqd.lame_lambda(MU, NU)
+    srv = eqd.Server(hbm_budget_bytes=int(150e9))
+    fes, weights = [], []
+    for h, (dz, Lf, Ln, w) in SERVE_GRIDS.items():
+        fe = eqd.FaultElasticity(eqd.bp8_grids(dz, Lf, Ln), lam, MU, Lf, device=device)
+        srv.add(fe, slots=512)
+        fe.h = h
+        fes.append(fe)
+        weights.append(w)
+    for fe in fes:  # first graph launches and tuning of every grid, untimed
+        srv.submit(fe, [fe.nf // 2 + fe.n2f // 2]).wait(900)
+    rng = np.random.default_rng(seed)
+    reqs, wall = run_mix(srv, fes, weights, rate, nreq, rng)
+    infos = [r.info() for r in reqs]
+    lat = np.array([i["latency"] for i in infos]) * 1e3
+    ncols = int(sum(i["ncols"] for i in infos))
+    span = max(i["t_done"] for i in infos) - min(i["t_submit"] for i in infos)
+    by_grid = {}
+    for r, i in zip(reqs, infos):
+        by_grid.setdefault(r.fe.h, []).append(i["latency"] * 1e3)
+    srv.close()
+    errs = []
+    chk = {}
+    for r in reqs[:check]:
+        if r.fe.h not in chk:
+            dz, Lf, Ln, _ = SERVE_GRIDS[r.fe.h]
+            chk[r.fe.h] = eqd.FaultElasticity(eqd.bp8_grids(dz, Lf, Ln), lam, MU, Lf, device=device,
+                                              precision="fp64", rtol=1e-12)
+        K64 = eqd.stiffness_columns(chk[r.fe.h], r.cols)[0]
+        errs.append(float(np.linalg.norm(r._out - K64) / np.linalg.norm(K64)))
+    for fe in chk.values():
+        fe.close()
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "columns_per_s": ncols / span, "requests": len(reqs), "columns": ncols,
+            "rate_req_s": rate, "unconverged": int(sum(i["unconverged"] for i in infos)),
+            "p50_ms_by_grid_h": {str(h): float(np.percentile(v, 50)) for h, v in sorted(by_grid.items())},
+            "p99_ms_by_grid_h": {str(h): float(np.percentile(v, 99)) for h, v in sorted(by_grid.items())},
+            "k_rel_err_max": max(errs) if errs else None, "k_rel_err_requests_checked": len(errs),
+            "what": "per-request latency, submit -> last K column in the request's host buffer"}
+
+
 def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -206,7 +289,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (unit slips)",
         "config": {"workload": wl, "sample_columns": int(len(cols)), "mean_iterations": float(np.mean(it))},
-        "cpu_baseline": {"value": v, "unit": "columns/s", "cores": nt, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "columns/s", "cores": nt, "cpu_model": cpu_model(), "kind": "port",
                          "sample": f"{len(cols)} seeded columns of the workload per step (C restatement of the "
                                    "reference column loop, assembled CSR A, FP64 Krylov-rule CG, OpenMP over columns)"},
         "e2e": {"value": v, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -304,11 +387,12 @@ def main():
     tms = (C.c_double * 16)()
     trows = (C.c_int32 * 16)()
     tthr = (C.c_int32 * 16)()
-    eqd._abi.check(lib.eqd_autotune(fe.handle, C.c_int32(min(len(cols), 512)), C.byref(sel), tms, trows, tthr,
-                                    C.byref(nv)))
+    # ncols = 0: report the choice the timed steps ran with (tuned on first use), no re-tuning.
+    eqd._abi.check(lib.eqd_autotune(fe.handle, C.c_int32(0), C.byref(sel), tms, trows, tthr, C.byref(nv)))
     autotune = {"selected": sel.value,
                 "variants": [{"tile_rows": trows[i], "threads": tthr[i], "ms_per_cg_iteration": tms[i]}
                              for i in range(nv.value)]}
+    kernel = apply_kernel_name(sel.value, n1, trows[sel.value], tthr[sel.value])
 
     # Roofline of the dominant kernel: FP32 stencil apply over the batch.
     ms = C.c_double()
@@ -321,7 +405,7 @@ def main():
     traffic = None
     tp = os.path.join(ROOT, "profiles", "apply_traffic.json")
     if os.path.exists(tp):
-        t = json.load(open(tp)).get(args.config)
+        t = json.load(open(tp)).get(args.config, {}).get(kernel.split("<")[0])
         if t:
             traffic = t["dram_bytes_per_launch_per_column"] * napply
 
@@ -411,6 +495,10 @@ def main():
     batched64_v = len(bcols) / st64.device_seconds
     b64.close()
 
+    serving = None
+    if world == 1 and args.serve_requests > 0:
+        serving = serving_leg(eqd, local, args.serve_requests, args.serve_rate)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         ofe, ref, ccols, nt = cpu_port_sample(args.config, n_cpu)
@@ -421,7 +509,7 @@ def main():
         t0 = time.perf_counter()
         ref.columns(ccols, nthreads=nt)
         cdt = time.perf_counter() - t0
-        cpu = {"value": len(ccols) / cdt, "unit": "columns/s", "cores": nt, "kind": "port",
+        cpu = {"value": len(ccols) / cdt, "unit": "columns/s", "cores": nt, "cpu_model": cpu_model(), "kind": "port",
                "sample": f"{len(ccols)} seeded columns of the workload, rtol 1e-10, OpenMP over columns "
                          "(C restatement of the reference column loop on the assembled CSR A)",
                "k_rel_err_vs_oracle_sample": o_err}
@@ -437,8 +525,8 @@ def main():
                    "mean_iterations": mean_it},
         "k_rel_err": {"frobenius_vs_fp64_rtol1e-12": k_err, "max_entry_vs_fp64_rtol1e-12": k_max,
                       "columns_checked": int(len(pick))},
-        "solve_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
-                     "what": "whole-batch build time per step"},
+        "step_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                    "what": "whole-K build time per step (all columns)"},
         "plain_fp64_single_rhs": {"value": plain_v, "unit": "columns/s",
                                   "latency_ms_p50": float(np.percentile(lat, 50)),
                                   "latency_ms_p99": float(np.percentile(lat, 99)),
@@ -447,7 +535,7 @@ def main():
         "speedup_vs_plain_fp64_single_rhs": value / plain_v,
         "speedup_vs_batched_fp64": value / batched64_v,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "plane_march_kernel<float,MODE_A>",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                      "peak_kind": peak_kind, "columns_per_launch": napply},
         "autotune": autotune,
         "e2e": e2e,
@@ -455,6 +543,8 @@ def main():
         "clocks": clocks,
         "wall_s_timed": wall,
     }
+    if serving:
+        line["serving"] = serving
     if gemv:
         line["gemv"] = gemv
     if toeplitz:

@@ -2026,6 +2026,41 @@ static void server_fail_all(eqd_server *S, int code, const std::string &msg) {
     S->cv_done.notify_all();
 }
 
+// Admission order of a grid's queued columns: the request with the fewest
+// columns still queued goes first (a small request is not held behind the
+// columns of a large one that arrived earlier), unless the oldest queued
+// request has waited longer than kServeAgeLimit seconds, which then goes
+// first (no request starves). A request's columns stay in submission order.
+// Queued columns of one request are contiguous in `pending` (submit appends
+// them under the server lock).
+constexpr double kServeAgeLimit = 2.0;
+
+static void take_columns(eqd_server *S, SrvGrid &g, int nfree, std::vector<ColWork> &take) {
+    struct Run {
+        size_t beg, len;
+        double t_submit;
+    };
+    while ((int)take.size() < nfree && !g.pending.empty()) {
+        std::vector<Run> runs;
+        for (size_t i = 0; i < g.pending.size();) {
+            const int64_t id = g.pending[i].tag >> kTagBits;
+            size_t j = i + 1;
+            while (j < g.pending.size() && (g.pending[j].tag >> kTagBits) == id) ++j;
+            auto it = S->reqs.find(id);
+            runs.push_back(Run{i, j - i, it != S->reqs.end() ? it->second->t_submit : 0.0});
+            i = j;
+        }
+        size_t pick = 0;  // runs[0] is the oldest
+        if (S->now() - runs[0].t_submit <= kServeAgeLimit)
+            for (size_t k = 1; k < runs.size(); ++k)
+                if (runs[k].len < runs[pick].len) pick = k;
+        const Run r = runs[pick];
+        const size_t n = std::min(r.len, (size_t)(nfree - (int)take.size()));
+        for (size_t k = 0; k < n; ++k) take.push_back(g.pending[r.beg + k]);
+        g.pending.erase(g.pending.begin() + (long)r.beg, g.pending.begin() + (long)(r.beg + n));
+    }
+}
+
 // One pass of a grid's worker: admit queued columns into free slots, run
 // the next graph of iterations, deliver the columns that finished.
 static int grid_pass(eqd_server *S, SrvGrid &g) {
@@ -2033,11 +2068,7 @@ static int grid_pass(eqd_server *S, SrvGrid &g) {
     std::vector<ColWork> take;
     {
         std::lock_guard<std::mutex> lk(S->mu);
-        const int nfree = g.free_slots();
-        while ((int)take.size() < nfree && !g.pending.empty()) {
-            take.push_back(g.pending.front());
-            g.pending.pop_front();
-        }
+        take_columns(S, g, g.free_slots(), take);
         const double t = S->now();
         for (const ColWork &c : take) {
             auto it = S->reqs.find(c.tag >> kTagBits);
