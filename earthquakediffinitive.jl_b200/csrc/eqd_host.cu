@@ -85,17 +85,41 @@ static constexpr int kNumVariants = 11;  // 9 plane-march variants, then 2 ring-
 static constexpr int kFirstRingVariant = 9;
 
 // Ring-march instances per n1: (x2 tile capacity, register cap per thread)
-// of its two variants. 136 registers hold a step without spills; a CTA's
-// threads x registers must stay within the SM's 65,536 (n1 = 33 takes fewer
-// registers and spills a little).
+// of its two variants. A CTA's threads x registers must fit the SM's 65,536,
+// with registers counted in units of 16 per thread (136 measured as too many
+// for 480 threads); 128 registers spill a few bytes.
 template <int N1> struct RingTraits;
-template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 136, T2B = 14, MB = 136; };
-template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 136, T2B = 10, MB = 136; };
-template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 120, T2B = 8, MB = 104; };
+template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 128, T2B = 14, MB = 128; };
+template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 128, T2B = 10, MB = 128; };
+template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 112, T2B = 8, MB = 96; };
 static_assert(ring_threads(9, RingTraits<9>::T2B) * RingTraits<9>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(21, RingTraits<21>::T2B) * RingTraits<21>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(33, RingTraits<33>::T2A) * RingTraits<33>::MA <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(33, RingTraits<33>::T2B) * RingTraits<33>::MB <= 65536, "ring CTA exceeds the register file");
+
+// The largest CTA the device will launch for a ring-march instance (its
+// register use included).
+template <int N1>
+static int ring_max_threads(int t2) {
+    using R = RingTraits<N1>;
+    cudaFuncAttributes fa{};
+    cudaError_t e = t2 == R::T2A ? cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2A, R::MA>)
+                                 : cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2B, R::MB>);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return fa.maxThreadsPerBlock;
+}
+
+static int ring_launchable_threads(int n1, int t2) {
+    switch (n1) {
+    case 9: return ring_max_threads<9>(t2);
+    case 21: return ring_max_threads<21>(t2);
+    case 33: return ring_max_threads<33>(t2);
+    default: return 0;
+    }
+}
 
 static int ring_t2_for(int n1, int which) {
     switch (n1) {
@@ -115,6 +139,10 @@ static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::strin
     }
     if (gc.n2 < 2 * kRingEdge) {
         why = "ring march: n2 below 14";
+        return false;
+    }
+    if (ring_threads(gc.n1, t2) > ring_launchable_threads(gc.n1, t2)) {
+        why = "ring march: the CTA does not fit the device's register file";
         return false;
     }
     const int m = gc.n2 - 2 * kRingEdge;
@@ -599,6 +627,7 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     if (rc) return rc;
     gc.nf = gc.n2f * gc.n3f;
 
+    CUDA_OR_RETURN(cudaSetDevice(d->device));  // launch limits below are queried for this device
     fill_op<float>(G->c32, gc, G->h);
     fill_op<double>(G->c64, gc, G->h);
     std::string why;
