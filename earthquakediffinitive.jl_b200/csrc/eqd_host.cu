@@ -73,6 +73,7 @@ struct MarchCfg {
     size_t smem = 0;
     size_t smem_af = 0;  // MODE_AF (second plane ring); 0: does not fit, the direction update runs apart
     int ring_t2 = 0;     // > 0: the FP32 A-apply runs ring_march_kernel with this x2 tile capacity
+    int ring_var = 0;    // which of the two ring-march instances of this n1 (0: A, 1: B)
     RingGeom rg{};
 };
 
@@ -89,9 +90,9 @@ static constexpr int kFirstRingVariant = 9;
 // with registers counted in units of 16 per thread (136 measured as too many
 // for 480 threads); 128 registers spill a few bytes.
 template <int N1> struct RingTraits;
-template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 128, T2B = 14, MB = 128; };
+template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 128, T2B = 7, MB = 96; };
 template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 128, T2B = 10, MB = 128; };
-template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 112, T2B = 8, MB = 96; };
+template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 96, T2B = 8, MB = 96; };
 static_assert(ring_threads(9, RingTraits<9>::T2B) * RingTraits<9>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(21, RingTraits<21>::T2B) * RingTraits<21>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(33, RingTraits<33>::T2A) * RingTraits<33>::MA <= 65536, "ring CTA exceeds the register file");
@@ -100,11 +101,11 @@ static_assert(ring_threads(33, RingTraits<33>::T2B) * RingTraits<33>::MB <= 6553
 // The largest CTA the device will launch for a ring-march instance (its
 // register use included).
 template <int N1>
-static int ring_max_threads(int t2) {
+static int ring_max_threads(int which) {
     using R = RingTraits<N1>;
     cudaFuncAttributes fa{};
-    cudaError_t e = t2 == R::T2A ? cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2A, R::MA>)
-                                 : cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2B, R::MB>);
+    cudaError_t e = which == 0 ? cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2A, R::MA>)
+                               : cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2B, R::MB>);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -112,11 +113,11 @@ static int ring_max_threads(int t2) {
     return fa.maxThreadsPerBlock;
 }
 
-static int ring_launchable_threads(int n1, int t2) {
+static int ring_launchable_threads(int n1, int which) {
     switch (n1) {
-    case 9: return ring_max_threads<9>(t2);
-    case 21: return ring_max_threads<21>(t2);
-    case 33: return ring_max_threads<33>(t2);
+    case 9: return ring_max_threads<9>(which);
+    case 21: return ring_max_threads<21>(which);
+    case 33: return ring_max_threads<33>(which);
     default: return 0;
     }
 }
@@ -132,7 +133,8 @@ static int ring_t2_for(int n1, int which) {
 
 // Launch configuration of ring_march_kernel: 7-row tiles at both x2 ends,
 // the rows between split into tiles of at most t2 rows.
-static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::string &why) {
+static bool make_ring_cfg(const GridConst &gc, const double h[3], int which, MarchCfg &out, std::string &why) {
+    const int t2 = ring_t2_for(gc.n1, which);
     if (t2 <= 0) {
         why = "ring march: n1 = " + std::to_string(gc.n1) + " has no specialised instance";
         return false;
@@ -141,7 +143,7 @@ static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::strin
         why = "ring march: n2 below 14";
         return false;
     }
-    if (ring_threads(gc.n1, t2) > ring_launchable_threads(gc.n1, t2)) {
+    if (ring_threads(gc.n1, t2) > ring_launchable_threads(gc.n1, which)) {
         why = "ring march: the CTA does not fit the device's register file";
         return false;
     }
@@ -149,6 +151,7 @@ static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::strin
     const int nmid = m > 0 ? (m + t2 - 1) / t2 : 0;
     out = MarchCfg{};
     out.ring_t2 = t2;
+    out.ring_var = which;
     out.rg.n2 = gc.n2;
     out.rg.n3 = gc.n3;
     out.rg.PS = gc.PS;
@@ -157,6 +160,33 @@ static bool make_ring_cfg(const GridConst &gc, int t2, MarchCfg &out, std::strin
     out.rg.nmid = std::max(nmid, 1);
     out.rg.drop_plane = -1;
     out.rg.poll_limit = 0;
+    {
+        const double lam = gc.lam, mu = gc.mu, lpm = gc.lam + gc.mu;
+        const double h2 = h[1], h3 = h[2], h2i = 1.0 / h2, h3i = 1.0 / h3;
+        RingScal &k = out.rg.k;
+        k.lam = (float)lam;
+        k.mu = (float)mu;
+        k.mu2 = (float)(2 * mu);
+        k.lpm = (float)lpm;
+        k.lpm_h2 = (float)(lpm * h2i);
+        k.lpm_h3 = (float)(lpm * h3i);
+        k.lam_h2 = (float)(lam * h2i);
+        k.lam_h3 = (float)(lam * h3i);
+        k.mu_h2 = (float)(mu * h2i);
+        k.mu_h3 = (float)(mu * h3i);
+        k.mu_h2s = (float)(mu * h2i * h2i);
+        k.mu2_h2s = (float)(2 * mu * h2i * h2i);
+        k.lam_h2s = (float)(lam * h2i * h2i);
+        k.mu_h3s = (float)(mu * h3i * h3i);
+        k.mu2_h3s = (float)(2 * mu * h3i * h3i);
+        k.lpm_h2h3 = (float)(lpm * h2i * h3i);
+        k.h3i = (float)h3i;
+        k.h2 = (float)h2;
+        k.h2s = (float)(h2 * h2);
+        k.h3 = (float)h3;
+        k.h3s = (float)(h3 * h3);
+        k.sat = (float)gc.sat_c;
+    }
     out.g.n1 = gc.n1;
     out.g.n2 = gc.n2;
     out.g.n3 = gc.n3;
@@ -402,11 +432,11 @@ static void launch_n1(int n1, dim3 grid, const MarchCfg &m, cudaStream_t st, con
 }
 
 template <int N1>
-static void launch_ring_n1(int t2, dim3 grid, const MarchCfg &m, const RingGeom &rg, cudaStream_t st,
+static void launch_ring_n1(int which, dim3 grid, const MarchCfg &m, const RingGeom &rg, cudaStream_t st,
                            const OpConst<float> &C, const float *in, float *out, const int8_t *status,
                            double *partials, unsigned *err) {
     using R = RingTraits<N1>;
-    if (t2 == R::T2A)
+    if (which == 0)
         ring_march_kernel<N1, R::T2A, R::MA><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
     else
         ring_march_kernel<N1, R::T2B, R::MB><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
@@ -426,9 +456,9 @@ static cudaError_t launch_ring(eqd_grid *G, const MarchCfg &m, const float *in, 
     const dim3 grid((unsigned)((long long)ncols * rg.ntiles));
     unsigned *err = G->err.as<unsigned>();
     switch (G->gc.n1) {
-    case 9: launch_ring_n1<9>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
-    case 21: launch_ring_n1<21>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
-    case 33: launch_ring_n1<33>(m.ring_t2, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    case 9: launch_ring_n1<9>(m.ring_var, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    case 21: launch_ring_n1<21>(m.ring_var, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
+    case 33: launch_ring_n1<33>(m.ring_var, grid, m, rg, st, G->c32, in, out, cs.status, partials, err); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -664,7 +694,7 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
                 // Ring-march variants: the BP8 lines (n1 = 9, 21, 33) only.
                 G->v32_maxt[v] = 0;
                 G->v32_lanes[v] = 1;
-                ok = make_ring_cfg(gc, ring_t2_for(gc.n1, v - kFirstRingVariant), G->v32[v], why);
+                ok = make_ring_cfg(gc, G->h, v - kFirstRingVariant, G->v32[v], why);
             }
             if (!ok) {
                 G->v32[v] = G->m32;  // fall back to the generic configuration

@@ -22,6 +22,11 @@
 //   * Component 2 finishes with component 3, three planes behind component 1:
 //     H23 = D1_2 v3 is then formed from the same x2 neighbours of plane p as
 //     the D2_2 v3 term, and a step reads only its own point of the newest plane.
+//   * The interior x2 and x3 stencils are exact rationals (instruction
+//     immediates) applied in unit spacing; 1/h and the Lame constants enter
+//     through a handful of per-grid products, and one branch per phase picks
+//     the interior or the closure form of all x3 derivatives. Idle lanes
+//     compute on in-range data with their stores predicated off.
 //   * Dot products p.q and p.p are accumulated in FP64 from FP64 products
 //     (in BP8 units a single product can exceed the FP32 range), then reduced
 //     per (column, tile) in a fixed order.
@@ -59,6 +64,30 @@ __host__ __device__ constexpr size_t ring_smem(int n1, int t2) {
     return kRingHeader + (size_t)kRing * 6 * ring_chunk(n1, t2) * 4 + (size_t)2 * 2 * (2 * t2 * n1) * 4;
 }
 
+// Interior stencils of the order-4 operators as exact rationals (unit
+// spacing): D1 = [1/12, -2/3, 0, 2/3, -1/12], D2 = [-1/12, 4/3, -5/2, 4/3,
+// -1/12], W = D1 D1 = [1/144, -1/9, 4/9, 1/9, -65/72, ...] (symmetric). The
+// ring march forms x2 and x3 derivatives in these raw units (the constants
+// are instruction immediates) and applies 1/h and the material constants
+// once, through the products below.
+constexpr float kD1a = 1.f / 12.f, kD1b = 2.f / 3.f;
+constexpr float kD2a = -1.f / 12.f, kD2b = 4.f / 3.f, kD2c = -5.f / 2.f;
+constexpr float kWa = 1.f / 144.f, kWb = -1.f / 9.f, kWc = 4.f / 9.f, kWd = 1.f / 9.f, kWe = -65.f / 72.f;
+
+// Per-grid scalars of the ring march: Lame constants times powers of the
+// inverse spacings h2i = 1/h2, h3i = 1/h3, and the spacings (closure rows,
+// which come from the tables in 1/h units, are converted to raw units).
+struct RingScal {
+    float lam, mu, mu2, lpm;                    // lambda, mu, 2 mu, lambda + mu
+    float lpm_h2, lpm_h3, lam_h2, lam_h3;       // (lambda + mu) h2i, ..., lambda h3i
+    float mu_h2, mu_h3;                         // mu h2i, mu h3i
+    float mu_h2s, mu2_h2s, lam_h2s;             // mu h2i^2, 2 mu h2i^2, lambda h2i^2
+    float mu_h3s, mu2_h3s;                      // mu h3i^2, 2 mu h3i^2
+    float lpm_h2h3, h3i;                        // (lambda + mu) h2i h3i, h3i
+    float h2, h2s, h3, h3s;                     // h2, h2^2, h3, h3^2
+    float sat;                                  // SAT scale c = 1 / (2 h1 w0)
+};
+
 struct RingGeom {
     int n2, n3, PS;
     long long colstride;
@@ -66,6 +95,7 @@ struct RingGeom {
     int nmid;             // middle tiles
     int drop_plane;       // test hook: the copy of this plane is never issued (-1: none)
     unsigned poll_limit;  // polls of a bounded wait before it gives up (0: the default bound)
+    RingScal k;
 };
 
 __device__ __forceinline__ bool ring_wait(uint64_t *bar, unsigned parity, unsigned *err, unsigned limit) {
@@ -151,7 +181,8 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
     }
     if (!valid) row = 0;  // idle lanes: every derived index stays inside the grid and the buffers
     const int i2 = a0 + row;
-    const unsigned facemask = __ballot_sync(0xffffffffu, is_face && valid);
+    is_face = is_face && valid;  // idle face-warp lanes take the regular path (and store nothing)
+    const unsigned facemask = __ballot_sync(0xffffffffu, is_face);
     const bool x2cl = i2 < 6 || i2 >= n2 - 6;
 
     // Zero the ring (rows outside the grid must read as zero), set up barriers.
@@ -215,7 +246,7 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
     const bool ff_x12 = (side == 0 && i1 == 0) || (side == 1 && i1 == N1 - 1) || i2 == 0 || i2 == n2 - 1;
     const float wq1 = (i1 < 4) ? A1.wq[i1] : (i1 >= N1 - 4 ? A1.wq[N1 - 1 - i1] : 1.f);
     const float wq2 = (i2 < 4) ? A2.wq[i2] : (i2 >= n2 - 4 ? A2.wq[n2 - 1 - i2] : 1.f);
-    const float hpt = ff_x12 ? 0.f : (float)(-C.hvol * (double)wq1 * (double)wq2);
+    const float hpt = (ff_x12 || !valid) ? 0.f : (float)(-C.hvol * (double)wq1 * (double)wq2);
 
     const int own = side * 3 * CH + i2 * N1 + i1 - base;   // component 1 of this point in a slot
     const int line = own - i1 + s1;                        // its x1 window
@@ -230,42 +261,46 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
 #pragma unroll
     for (int k = 0; k < 4; ++k) w2q[k] = w3q[k] = 0.f;
     double acc0 = 0.0, acc1 = 0.0;
-    const float lam = C.lam, mu = C.mu, lpm = C.lpm, sat = C.sat_c;
+    const RingScal K = g.k;
     const float sgn = side == 0 ? -1.f : 1.f;
     const int s_end = n3 + 6;
     int dead_at = -1;
 
-    // x3 first and second derivatives at plane q from a window whose slot
-    // for plane q is Q (compile time); closure planes use the table row r.
-    auto x3d1 = [&](const float (&w)[kRing], auto Qc, bool interior, int r) -> float {
+    // Raw (unit-spacing) x3 first and second derivatives at the plane whose
+    // window slot is Q: interior planes use the rational stencils, the
+    // closure planes (table row r, in 1/h units) are converted to raw units.
+    auto x3d1i = [&](const float (&w)[kRing], auto Qc) -> float {
         constexpr int Q = decltype(Qc)::value;
-        if (interior)
-            return A3.d1_int[0] * w[(Q - 2) & 7] + A3.d1_int[1] * w[(Q - 1) & 7] + A3.d1_int[3] * w[(Q + 1) & 7] +
-                   A3.d1_int[4] * w[(Q + 2) & 7];
+        return kD1a * (w[(Q - 2) & 7] - w[(Q + 2) & 7]) + kD1b * (w[(Q + 1) & 7] - w[(Q - 1) & 7]);
+    };
+    auto x3d2i = [&](const float (&w)[kRing], auto Qc) -> float {
+        constexpr int Q = decltype(Qc)::value;
+        return kD2a * (w[(Q - 2) & 7] + w[(Q + 2) & 7]) + kD2b * (w[(Q - 1) & 7] + w[(Q + 1) & 7]) + kD2c * w[Q & 7];
+    };
+    auto x3d1c = [&](const float (&w)[kRing], auto Qc, int r) -> float {
+        constexpr int Q = decltype(Qc)::value;
         float s = 0.f;
 #pragma unroll
         for (int o = 0; o < 7; ++o) s += A3.d1_cl[r][o] * w[(Q - 3 + o) & 7];
-        return s;
+        return s * K.h3;
     };
-    auto x3d2 = [&](const float (&w)[kRing], auto Qc, bool interior, int r) -> float {
+    auto x3d2c = [&](const float (&w)[kRing], auto Qc, int r) -> float {
         constexpr int Q = decltype(Qc)::value;
-        if (interior)
-            return A3.d2_int[0] * w[(Q - 2) & 7] + A3.d2_int[1] * w[(Q - 1) & 7] + A3.d2_int[2] * w[Q & 7] +
-                   A3.d2_int[3] * w[(Q + 1) & 7] + A3.d2_int[4] * w[(Q + 2) & 7];
         float s = 0.f;
 #pragma unroll
         for (int o = 0; o < 7; ++o) s += A3.d2_cl[r][o] * w[(Q - 3 + o) & 7];
-        return s;
+        return s * K.h3s;
     };
+    // Quadrature weight of x3 plane q; zero on the far-field planes.
     auto plane_w = [&](int q) -> float {
-        if (q <= 0 || q >= n3 - 1) return 0.f;
-        if (q < 4) return A3.wq[q];
-        if (q >= n3 - 4) return A3.wq[n3 - 1 - q];
-        return 1.f;
+        const int m = min(q, n3 - 1 - q);
+        return m <= 0 ? 0.f : (m < 4 ? A3.wq[m] : 1.f);
     };
 
     // One march step s (slot U = s mod 8): ingest plane s; in-plane work and
     // component 1 of plane p = s - 3; components 2, 3 of plane z = s - 6.
+    // Idle lanes compute on in-range data and store nothing (their H weight
+    // is zero and their stores and sums are predicated off).
     auto step = [&](auto Uc, int s) -> bool {
         constexpr int U = decltype(Uc)::value;
         constexpr int UP = (U + kRing - 3) & 7;   // slot of plane p
@@ -277,12 +312,10 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
         float a = 0.f, b = 0.f, c = 0.f;
         if (s < n3) {
             if (!ring_wait(&mbar[U], (unsigned)(s >> 3) & 1u, err, g.poll_limit)) s_dead[BUF] = 1;
-            if (valid) {
-                const float *pl = ring + U * SLOT + own;
-                a = pl[0];
-                b = pl[CH];
-                c = pl[2 * CH];
-            }
+            const float *pl = ring + U * SLOT + own;
+            a = pl[0];
+            b = pl[CH];
+            c = pl[2 * CH];
         }
         v1w[U] = a;
         v2w[U] = b;
@@ -291,14 +324,13 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
         // ---- in-plane work at p ----------------------------------------------
         const int p = s - 3;
         const bool pin = p >= 0 && p < n3;
-        const bool x3i = p >= 4 && p <= n3 - 5;
-        const int r3 = p < 4 ? p : 4 + (n3 - 1 - p);
-        float w1 = 0.f, w2p = 0.f, w3p = 0.f, F3 = 0.f, H23 = 0.f;
-        if (valid && pin) {
+        float w1 = 0.f, w2p = 0.f, w3p = 0.f, F3 = 0.f, h23r = 0.f;
+        if (pin) {
             const float *pl = ring + UP * SLOT;
             const float *o1 = pl + own, *o2 = o1 + CH, *o3 = o2 + CH;
             const float *l1 = pl + line, *l2 = l1 + CH, *l3 = l2 + CH;
             const float v1 = v1w[UP], v2 = v2w[UP], v3 = v3w[UP];
+            // x1 (per-thread rows, 1/h units)
             float G1 = 0.f, A11 = 0.f, A21 = 0.f, A31 = 0.f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
@@ -308,30 +340,57 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
                 A21 += c2[k] * xb;
                 A31 += c2[k] * xc;
             }
-            float G2 = x2_d1i(A2, o2, N1);
-            float H21 = x2_d1i(A2, o1, N1);
-            H23 = x2_d1i(A2, o3, N1);
-            float A12 = x2_d2i(A2, o1, v1, N1);
-            float A22 = x2_d2i(A2, o2, v2, N1);
-            float A32 = x2_d2i(A2, o3, v3, N1);
-            float W2 = x2_wi(A2, o2, v2, N1);
+            // x2 (raw units): sums and differences of the neighbour pairs
+            const float a_m2 = o1[-2 * N1], a_m1 = o1[-N1], a_p1 = o1[N1], a_p2 = o1[2 * N1];
+            const float b_m4 = o2[-4 * N1], b_m3 = o2[-3 * N1], b_m2 = o2[-2 * N1], b_m1 = o2[-N1];
+            const float b_p1 = o2[N1], b_p2 = o2[2 * N1], b_p3 = o2[3 * N1], b_p4 = o2[4 * N1];
+            const float c_m2 = o3[-2 * N1], c_m1 = o3[-N1], c_p1 = o3[N1], c_p2 = o3[2 * N1];
+            float h21r = kD1a * (a_m2 - a_p2) + kD1b * (a_p1 - a_m1);
+            float a12r = kD2a * (a_m2 + a_p2) + kD2b * (a_m1 + a_p1) + kD2c * v1;
+            const float bs1 = b_m1 + b_p1, bs2 = b_m2 + b_p2;
+            float g2r = kD1a * (b_m2 - b_p2) + kD1b * (b_p1 - b_m1);
+            float a22r = kD2a * bs2 + kD2b * bs1 + kD2c * v2;
+            float w2r = kWa * (b_m4 + b_p4) + kWb * (b_m3 + b_p3) + kWc * bs2 + kWd * bs1 + kWe * v2;
+            h23r = kD1a * (c_m2 - c_p2) + kD1b * (c_p1 - c_m1);
+            float a32r = kD2a * (c_m2 + c_p2) + kD2b * (c_m1 + c_p1) + kD2c * v3;
             if (x2cl) {
+                // closure rows: table corrections (1/h units) converted to raw units
                 const X2Corr gdd = x2_geom(i2, N1, n2, 4);
                 const X2Corr gw = x2_geom(i2, N1, n2, 6);
-                x2_corr_dd(A2, gdd, o1, H21, A12);
-                x2_corr_dd(A2, gdd, o2, G2, A22);
-                x2_corr_dd(A2, gdd, o3, H23, A32);
-                x2_corr_w(A2, gw, o2, W2);
+                float e_h21 = 0.f, e_a12 = 0.f, e_g2 = 0.f, e_a22 = 0.f, e_h23 = 0.f, e_a32 = 0.f, e_w2 = 0.f;
+                x2_corr_dd(A2, gdd, o1, e_h21, e_a12);
+                x2_corr_dd(A2, gdd, o2, e_g2, e_a22);
+                x2_corr_dd(A2, gdd, o3, e_h23, e_a32);
+                x2_corr_w(A2, gw, o2, e_w2);
+                h21r += e_h21 * K.h2;
+                g2r += e_g2 * K.h2;
+                h23r += e_h23 * K.h2;
+                a12r += e_a12 * K.h2s;
+                a22r += e_a22 * K.h2s;
+                a32r += e_a32 * K.h2s;
+                w2r += e_w2 * K.h2s;
             }
-            const float G3 = x3d1(v3w, IC<UP>{}, x3i, r3);
-            const float A13 = x3d2(v1w, IC<UP>{}, x3i, r3);
-            const float A23 = x3d2(v2w, IC<UP>{}, x3i, r3);
-            const float A33 = x3d2(v3w, IC<UP>{}, x3i, r3);
-            const float F1 = lam * G1 + lpm * (G2 + G3);
-            F3 = lam * G3 + lpm * (G1 + G2);
-            w1 = mu * (2.f * A11 + A12 + A13);
-            w2p = mu * (A21 + 2.f * A22 + A23) + lam * W2;
-            w3p = mu * (A31 + A32 + 2.f * A33);
+            // x3 (raw units), one branch for all five
+            float g3r, a13r, a23r, a33r, d3v1r;
+            if (p >= 4 && p <= n3 - 5) {
+                g3r = x3d1i(v3w, IC<UP>{});
+                a13r = x3d2i(v1w, IC<UP>{});
+                a23r = x3d2i(v2w, IC<UP>{});
+                a33r = x3d2i(v3w, IC<UP>{});
+                d3v1r = x3d1i(v1w, IC<UP>{});
+            } else {
+                const int r3 = p < 4 ? p : 4 + (n3 - 1 - p);
+                g3r = x3d1c(v3w, IC<UP>{}, r3);
+                a13r = x3d2c(v1w, IC<UP>{}, r3);
+                a23r = x3d2c(v2w, IC<UP>{}, r3);
+                a33r = x3d2c(v3w, IC<UP>{}, r3);
+                d3v1r = x3d1c(v1w, IC<UP>{}, r3);
+            }
+            const float F1 = K.lam * G1 + K.lpm_h2 * g2r + K.lpm_h3 * g3r;
+            F3 = K.lam_h3 * g3r + K.lpm * G1 + K.lpm_h2 * g2r;
+            w1 = K.mu2 * A11 + K.mu_h2s * a12r + K.mu_h3s * a13r;
+            w2p = K.mu * A21 + K.mu2_h2s * a22r + K.mu_h3s * a23r + K.lam_h2s * w2r;
+            w3p = K.mu * A31 + K.mu_h2s * a32r + K.mu2_h3s * a33r;
             if (is_face) {
                 // Traction on the fixed +x1 axis and SAT c (tau+ - tau-) on both
                 // faces; the other side of the node is the adjacent lane. The
@@ -345,22 +404,24 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
                     dh2 += cd * l2[k];
                     dh3 += cd * l3[k];
                 }
-                const float D3v1 = x3d1(v1w, IC<UP>{}, x3i, r3);
-                const float tau1 = lam * (G1 + G2 + G3) + 2.f * mu * dh1;
-                const float tau2 = mu * (H21 + dh2);
-                const float tau3 = mu * (D3v1 + dh3);
+                const float tau1 = K.lam * G1 + K.lam_h2 * g2r + K.lam_h3 * g3r + K.mu2 * dh1;
+                const float tau2 = K.mu_h2 * h21r + K.mu * dh2;
+                const float tau3 = K.mu_h3 * d3v1r + K.mu * dh3;
                 const float o1t = __shfl_xor_sync(facemask, tau1, 1);
                 const float o2t = __shfl_xor_sync(facemask, tau2, 1);
                 const float o3t = __shfl_xor_sync(facemask, tau3, 1);
-                w1 += sat * sgn * (tau1 - o1t);
-                w2p += sat * sgn * (tau2 - o2t);
-                w3p += sat * sgn * (tau3 - o3t);
+                const float cs = K.sat * sgn;
+                w1 += cs * (tau1 - o1t);
+                w2p += cs * (tau2 - o2t);
+                w3p += cs * (tau3 - o3t);
             }
-            xF1[BUF * NPT + pidx] = F1;
-            xH21[BUF * NPT + pidx] = H21;
+            if (valid) {
+                xF1[BUF * NPT + pidx] = F1;
+                xH21[BUF * NPT + pidx] = h21r;
+            }
         }
         F3w[UP] = F3;
-        H23w[UP] = H23;
+        H23w[UP] = h23r;
         __syncthreads();
         if (s_dead[BUF]) {
             dead_at = s;
@@ -373,45 +434,56 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
         }
 
         // ---- component 1 of p; components 2, 3 of p enter the queue ------------
-        if (valid && pin) {
+        if (pin) {
             const float *xf = xF1 + BUF * NPT + pline;
             const float *xh = xH21 + BUF * NPT + pline;
-            float E1 = 0.f, E21 = 0.f;
+            float E1 = 0.f, e21r = 0.f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
                 E1 += c1[k] * xf[k];
-                E21 += c1[k] * xh[k];
+                e21r += c1[k] * xh[k];
             }
             float u1 = w1 + E1;
             if (is_face) u1 = 0.5f * (u1 + __shfl_xor_sync(facemask, u1, 1));
             const float y1 = hpt * plane_w(p) * u1;
-            ocol[(long long)p * g.PS] = y1;
-            const double v1 = (double)v1w[UP];
-            acc0 = fma(v1, (double)y1, acc0);
-            acc1 = fma(v1, v1, acc1);
-            w2q[QP] = w2p + lpm * E21;
+            if (valid) {
+                ocol[(long long)p * g.PS] = y1;
+                const double v1 = (double)v1w[UP];
+                acc0 = fma(v1, (double)y1, acc0);
+                acc1 = fma(v1, v1, acc1);
+            }
+            w2q[QP] = w2p + K.lpm_h2 * e21r;
             w3q[QP] = w3p;
         }
         // ---- components 2, 3 of z ----------------------------------------------
         const int z = s - 6;
-        if (valid && z >= 0 && z < n3) {
-            const bool x3iz = z >= 4 && z <= n3 - 5;
-            const int r3z = z < 4 ? z : 4 + (n3 - 1 - z);
-            float u2 = w2q[QZ] + lpm * x3d1(H23w, IC<UZ>{}, x3iz, r3z);
-            float u3 = w3q[QZ] + x3d1(F3w, IC<UZ>{}, x3iz, r3z);
+        if (z >= 0 && z < n3) {
+            float dh, df;
+            if (z >= 4 && z <= n3 - 5) {
+                dh = x3d1i(H23w, IC<UZ>{});
+                df = x3d1i(F3w, IC<UZ>{});
+            } else {
+                const int r3z = z < 4 ? z : 4 + (n3 - 1 - z);
+                dh = x3d1c(H23w, IC<UZ>{}, r3z);
+                df = x3d1c(F3w, IC<UZ>{}, r3z);
+            }
+            float u2 = w2q[QZ] + K.lpm_h2h3 * dh;
+            float u3 = w3q[QZ] + K.h3i * df;
             if (is_face) {
                 u2 = 0.5f * (u2 + __shfl_xor_sync(facemask, u2, 1));
                 u3 = 0.5f * (u3 + __shfl_xor_sync(facemask, u3, 1));
             }
             const float hw = hpt * plane_w(z);
             const float y2 = hw * u2, y3 = hw * u3;
-            ocol[cstr + (long long)z * g.PS] = y2;
-            ocol[2 * cstr + (long long)z * g.PS] = y3;
-            const double v2 = (double)v2w[UZ], v3 = (double)v3w[UZ];
-            acc0 = fma(v2, (double)y2, acc0);
-            acc0 = fma(v3, (double)y3, acc0);
-            acc1 = fma(v2, v2, acc1);
-            acc1 = fma(v3, v3, acc1);
+            if (valid) {
+                ocol[cstr + (long long)z * g.PS] = y2;
+                ocol[2 * cstr + (long long)z * g.PS] = y3;
+                const double v2 = (double)v2w[UZ], v3 = (double)v3w[UZ];
+                acc0 = fma(v2, (double)y2, acc0);
+                acc0 = fma(v3, (double)y3, acc0);
+                acc1 = fma(v2, v2, acc1);
+                acc1 = fma(v3, v3, acc1);
+            }
         }
         return true;
     };
