@@ -90,9 +90,11 @@ static constexpr int kFirstRingVariant = 9;
 // with registers counted in units of 16 per thread (136 measured as too many
 // for 480 threads); 128 registers spill a few bytes.
 template <int N1> struct RingTraits;
-template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 128, T2B = 7, MB = 96; };
-template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 128, T2B = 10, MB = 128; };
-template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 96, T2B = 8, MB = 96; };
+// Variant A unrolls the march over the ring; variant B is the same tile
+// without the unrolling (DYN: smaller code, window moves).
+template <> struct RingTraits<9> { static constexpr int T2A = 7, MA = 128, T2B = 7, MB = 128; };
+template <> struct RingTraits<21> { static constexpr int T2A = 7, MA = 128, T2B = 7, MB = 128; };
+template <> struct RingTraits<33> { static constexpr int T2A = 7, MA = 96, T2B = 7, MB = 96; };
 static_assert(ring_threads(9, RingTraits<9>::T2B) * RingTraits<9>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(21, RingTraits<21>::T2B) * RingTraits<21>::MB <= 65536, "ring CTA exceeds the register file");
 static_assert(ring_threads(33, RingTraits<33>::T2A) * RingTraits<33>::MA <= 65536, "ring CTA exceeds the register file");
@@ -105,7 +107,7 @@ static int ring_max_threads(int which) {
     using R = RingTraits<N1>;
     cudaFuncAttributes fa{};
     cudaError_t e = which == 0 ? cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2A, R::MA>)
-                               : cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2B, R::MB>);
+                               : cudaFuncGetAttributes(&fa, ring_march_kernel<N1, R::T2B, R::MB, true>);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -439,7 +441,8 @@ static void launch_ring_n1(int which, dim3 grid, const MarchCfg &m, const RingGe
     if (which == 0)
         ring_march_kernel<N1, R::T2A, R::MA><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
     else
-        ring_march_kernel<N1, R::T2B, R::MB><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials, err);
+        ring_march_kernel<N1, R::T2B, R::MB, true><<<grid, m.threads, m.smem, st>>>(C, rg, in, out, status, partials,
+                                                                                     err);
 }
 
 // The FP32 CG apply through ring_march_kernel (one CTA per column and x2
@@ -537,7 +540,7 @@ static cudaError_t configure_kernels(int smem_max) {
         (const void *)plane_march_kernel<double, double, MODE_AF, kMaxT64b, N, 1>,
 #define EQD_RING_KS(N)                                                                                     \
     (const void *)ring_march_kernel<N, RingTraits<N>::T2A, RingTraits<N>::MA>,                             \
-        (const void *)ring_march_kernel<N, RingTraits<N>::T2B, RingTraits<N>::MB>,
+        (const void *)ring_march_kernel<N, RingTraits<N>::T2B, RingTraits<N>::MB, true>,
     const void *ks[] = {
         EQD_FOR_N1(EQD_KS) EQD_KS(0)
         (const void *)plane_march_kernel<float, float, MODE_AP, kMaxT32, 0, 1>,

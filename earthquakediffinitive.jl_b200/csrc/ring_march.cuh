@@ -110,8 +110,11 @@ template <int N>
 using IC = std::integral_constant<int, N>;
 
 // REGS caps the registers of a thread (with the CTA size, how many CTAs
-// share an SM).
-template <int N1, int T2, int REGS>
+// share an SM). DYN: the march is not unrolled; every step runs the code of
+// slot 0 with ring slots, mbarrier and exchange buffer chosen at run time,
+// and the register windows rotate by one entry after each step (a smaller
+// code body at the price of the window moves).
+template <int N1, int T2, int REGS, bool DYN = false>
 __global__ void __maxnreg__(REGS)
 ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constant__ RingGeom g,
                   const float *__restrict__ in, float *__restrict__ out, const int8_t *__restrict__ status,
@@ -303,16 +306,18 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
     // is zero and their stores and sums are predicated off).
     auto step = [&](auto Uc, int s) -> bool {
         constexpr int U = decltype(Uc)::value;
-        constexpr int UP = (U + kRing - 3) & 7;   // slot of plane p
-        constexpr int UZ = (U + kRing - 6) & 7;   // slot of plane z
-        constexpr int BUF = U & 1;
+        constexpr int UP = (U + kRing - 3) & 7;   // window slot of plane p
+        constexpr int UZ = (U + kRing - 6) & 7;   // window slot of plane z
+        const int RS = DYN ? (s & 7) : U;         // ring slot / mbarrier of plane s
+        const int RP = DYN ? ((s + kRing - 3) & 7) : UP;  // ring slot of plane p
+        const int BUF = DYN ? (s & 1) : (U & 1);
         constexpr int QP = (U + 1) & 3;           // queue entry of plane p  (p = s - 3)
         constexpr int QZ = (U + 2) & 3;           // queue entry of plane z  (z = s - 6)
         // ---- ingest plane s: the own point's three components ----------------
         float a = 0.f, b = 0.f, c = 0.f;
         if (s < n3) {
-            if (!ring_wait(&mbar[U], (unsigned)(s >> 3) & 1u, err, g.poll_limit)) s_dead[BUF] = 1;
-            const float *pl = ring + U * SLOT + own;
+            if (!ring_wait(&mbar[RS], (unsigned)(s >> 3) & 1u, err, g.poll_limit)) s_dead[BUF] = 1;
+            const float *pl = ring + RS * SLOT + own;
             a = pl[0];
             b = pl[CH];
             c = pl[2 * CH];
@@ -326,7 +331,7 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
         const bool pin = p >= 0 && p < n3;
         float w1 = 0.f, w2p = 0.f, w3p = 0.f, F3 = 0.f, h23r = 0.f;
         if (pin) {
-            const float *pl = ring + UP * SLOT;
+            const float *pl = ring + RP * SLOT;
             const float *o1 = pl + own, *o2 = o1 + CH, *o3 = o2 + CH;
             const float *l1 = pl + line, *l2 = l1 + CH, *l3 = l2 + CH;
             const float v1 = v1w[UP], v2 = v2w[UP], v3 = v3w[UP];
@@ -489,7 +494,34 @@ ring_march_kernel(const __grid_constant__ OpConst<float> C, const __grid_constan
     };
 
     bool alive = true;
-    for (int s0 = 0; s0 < s_end && alive; s0 += kRing) {
+    if constexpr (DYN) {
+        // Slot 0 holds the newest plane; after a step every window moves one
+        // entry toward older planes (slot k -> slot k - 1 mod 8).
+        auto rot8 = [](float (&w)[kRing]) {
+            const float t = w[0];
+#pragma unroll
+            for (int k = 0; k < kRing - 1; ++k) w[k] = w[k + 1];
+            w[kRing - 1] = t;
+        };
+        auto rot4 = [](float (&w)[4]) {
+            const float t = w[0];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) w[k] = w[k + 1];
+            w[3] = t;
+        };
+#pragma unroll 1
+        for (int s = 0; s < s_end && alive; ++s) {
+            alive = step(IC<0>{}, s);
+            rot8(v1w);
+            rot8(v2w);
+            rot8(v3w);
+            rot8(F3w);
+            rot8(H23w);
+            rot4(w2q);
+            rot4(w3q);
+        }
+    }
+    for (int s0 = 0; s0 < s_end && alive && !DYN; s0 += kRing) {
 #define EQD_RING_STEP(U) \
     if (alive && s0 + U < s_end) alive = step(IC<U>{}, s0 + U);
         EQD_RING_STEP(0)

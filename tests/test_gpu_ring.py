@@ -46,7 +46,7 @@ def is_ring(eqd, fe, variant):
     """The variant's reported CTA size is the ring kernel's (a variant falls
     back to the generic plane march on grids the ring kernel does not cover)."""
     n1 = fe.grids.n1
-    t2 = {9: (7, 7), 21: (7, 10), 33: (7, 8)}[n1][variant - RING_VARIANTS[0]]
+    t2 = 7
     r32 = lambda x: (x + 31) // 32 * 32
     _, table = eqd.autotune(fe, 4)
     return table[variant][1] == 2 * r32(t2 * n1) + r32(2 * t2)
