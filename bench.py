@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=48, help="requests of the serving mix (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the serving mix (req/s)")
+    ap.add_argument("--columns", type=int, default=0,
+                    help="build only the first N columns of the workload (profiler captures of a smaller case; "
+                         "0: all)")
     return ap.parse_args()
 
 
@@ -311,6 +314,8 @@ def main():
     wl, n1, n23, nf = workload_name(args.config)
     n_err, n_plain, n_b64, n_cpu = SAMPLES[args.config]
     all_cols = workload_columns(args.config, nf)
+    if args.columns > 0:
+        all_cols = all_cols[: args.columns]
     ncols = len(all_cols)
     lo, hi = shard_range(ncols, rank, world)
     cols = all_cols[lo:hi]
