@@ -442,6 +442,28 @@ def main():
                 "rel_err_vs_host": float(np.linalg.norm(y.cpu().numpy() - yref) / np.linalg.norm(yref)),
                 "slip": "N(0, 1 m^2), default_rng(0)"}
 
+    # Batched K S for 64 slip vectors (Runge-Kutta stages / ensembles): the
+    # blocked path reads K once per 64 vectors. Timed through the host API
+    # (slips in, tractions out, every call).
+    gemm = None
+    if ncols == 2 * nf:
+        n = 2 * nf
+        nv = 64
+        Sm = np.random.default_rng(2).standard_normal((n, nv))
+        KM = eqd.KMatrix(Kmix)
+        KM.gemv(Sm)
+        reps = 5
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            Ym = KM.gemv(Sm)
+        gdt = (time.perf_counter() - t0) / reps
+        KM.close()
+        Yref = Kmix @ Sm
+        gemm = {"n": n, "nvec": nv, "ms": gdt * 1e3, "GFLOP_s": 2.0 * n * n * nv / gdt / 1e9,
+                "K_GB_s": 8.0 * n * n / gdt / 1e9,
+                "rel_err_vs_host": float(np.linalg.norm(Ym - Yref) / np.linalg.norm(Yref)),
+                "what": "eqd_kmat_gemv with 64 vectors through the host API (copies of S and Y included)"}
+
     # The Toeplitz mode's 10 source solves (src/FaultResponse.jl:339-393:
     # the centre node, then the four corners, each with s2 and s3) on the
     # large grid, batched, checked against FP64 single-RHS CG.
@@ -552,6 +574,8 @@ def main():
         line["serving"] = serving
     if gemv:
         line["gemv"] = gemv
+    if gemm:
+        line["batched_ks"] = gemm
     if toeplitz:
         line["toeplitz"] = toeplitz
     if cpu:

@@ -1968,10 +1968,39 @@ static int gemv_slices(int n) {
     return std::min(s, std::max(1, n / 64));
 }
 
+// Vectors from which y = K s runs as the blocked K S (K read once per 64
+// vectors) instead of the GEMV (K read once per 4 vectors).
+static constexpr int kGemmMinVectors = 8;
+
+// Column slices of the blocked K S: enough CTAs for two per SM, each slice
+// at least 256 columns of K.
+static int gemm_slices(int n, int nvec) {
+    const long long tiles = (long long)((n + kGemmBM - 1) / kGemmBM) * ((nvec + kGemmBN - 1) / kGemmBN);
+    const long long want = (2LL * 148 + tiles - 1) / tiles;
+    return (int)std::max<long long>(1, std::min<long long>(want, std::max(1, n / 256)));
+}
+
 extern "C" int eqd_kmat_gemv(eqd_kmat *M, const double *s, double *y, int32_t nvec) {
     if (!M || !s || !y || nvec < 1) return fail(EQD_ERR_ARG, "invalid argument");
     CUDA_OR_RETURN(cudaSetDevice(M->device));
     const int n = M->n;
+    if (nvec >= kGemmMinVectors) {
+        const int ns = gemm_slices(n, nvec);
+        CUDA_OR_RETURN(M->s.ensure(sizeof(double) * (size_t)n * nvec));
+        CUDA_OR_RETURN(M->y.ensure(sizeof(double) * (size_t)n * nvec));
+        CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)n * nvec * ns));
+        CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, sizeof(double) * (size_t)n * nvec, cudaMemcpyHostToDevice, M->stream));
+        const dim3 grid((unsigned)((n + kGemmBM - 1) / kGemmBM), (unsigned)ns, (unsigned)((nvec + kGemmBN - 1) / kGemmBN));
+        gemm_ks_partial_kernel<<<grid, 256, 0, M->stream>>>(M->K.as<double>(), M->s.as<double>(), n, ns, nvec,
+                                                             M->part.as<double>());
+        const long long ne = (long long)n * nvec;
+        gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, M->stream>>>(M->part.as<double>(), n, ns, nvec,
+                                                                               M->y.as<double>());
+        CUDA_OR_RETURN(cudaGetLastError());
+        CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, sizeof(double) * (size_t)n * nvec, cudaMemcpyDeviceToHost, M->stream));
+        CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
+        return EQD_OK;
+    }
     const int nslice = gemv_slices(n);
     CUDA_OR_RETURN(M->s.ensure(sizeof(double) * (size_t)n * nvec));
     CUDA_OR_RETURN(M->y.ensure(sizeof(double) * (size_t)n * nvec));

@@ -862,6 +862,74 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Blocked FP64 K S for many slip vectors (Runge-Kutta stages, ensembles):
+// K is read once per 64 vectors instead of once per 4. CTA tile: 64 rows of
+// K x 64 vectors over the k-range of one column slice, in steps of 16 columns
+// staged in shared memory; each of the 256 threads accumulates a 4 x 4 block
+// (rows ty + 16 i, vectors tx + 16 j) in a fixed k order. Partial sums go to
+// part[(v * nslice + slice) * n + row], the GEMV's layout, and the same
+// fixed-order reduction over slices finishes them.
+// ---------------------------------------------------------------------------
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16;
+
+__global__ void __launch_bounds__(256) gemm_ks_partial_kernel(const double *__restrict__ K,
+                                                              const double *__restrict__ S, long long n, int nslice,
+                                                              int nvec, double *__restrict__ part) {
+    __shared__ double As[kGemmBK][kGemmBM + 1];
+    __shared__ double Bs[kGemmBK][kGemmBN + 1];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const long long row0 = (long long)blockIdx.x * kGemmBM;
+    const int slice = blockIdx.y;
+    const int v0 = blockIdx.z * kGemmBN;
+    const long long c0 = n * slice / nslice, c1 = n * (slice + 1) / nslice;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (long long k0 = c0; k0 < c1; k0 += kGemmBK) {
+        // K tile: rows row0 .. row0 + 63 (contiguous in a column), 16 columns
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = tid % kGemmBM, kk = tid / kGemmBM + 4 * q;
+            const long long row = row0 + r, c = k0 + kk;
+            As[kk][r] = (row < n && c < c1) ? K[c * n + row] : 0.0;
+        }
+        // S tile: 16 consecutive entries of each of 64 vectors
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int kk = tid % kGemmBK, j = tid / kGemmBK + 16 * q;
+            const long long c = k0 + kk;
+            Bs[kk][j] = (c < c1 && v0 + j < nvec) ? S[(long long)(v0 + j) * n + c] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kGemmBK; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const long long row = row0 + ty + 16 * i;
+        if (row >= n) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int v = v0 + tx + 16 * j;
+            if (v < nvec) part[((long long)v * nslice + slice) * n + row] = acc[i][j];
+        }
+    }
+}
+
 __global__ void gemv_reduce_kernel(const double *__restrict__ part, long long n, int nslice, int nvec,
                                    double *__restrict__ y) {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;

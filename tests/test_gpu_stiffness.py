@@ -150,6 +150,21 @@ def test_bp8_dz100_model(eqd):
     assert rel(K, K_ref) < K_TOL
 
 
+@pytest.mark.parametrize("n, nvec", [(578, 8), (1155, 64), (2178, 70)])
+def test_batched_ks(eqd, n, nvec):
+    """y = K S for many slip vectors (the blocked K S path, K read once per
+    64 vectors) against numpy FP64, relative to |K||S|."""
+    rng = np.random.default_rng(n)
+    K = rng.standard_normal((n, n))
+    S = rng.standard_normal((n, nvec))
+    M = eqd.KMatrix(K)
+    Y = M.gemv(S)
+    M.close()
+    scale = abs(K).dot(abs(S)).max()
+    assert Y.shape == (n, nvec)
+    assert abs(Y - K @ S).max() <= 1e-13 * scale
+
+
 def test_gemv(eqd):
     rng = np.random.default_rng(0)
     n = 578
