@@ -28,7 +28,6 @@ EQD_PRECOND_JACOBI = 1
 EQD_FLAG_STRICT = 1
 EQD_FLAG_NO_SPLIT = 2
 EQD_FLAG_FUSE = 4
-EQD_FLAG_UNGATED = 8
 
 COL_CONVERGED = 1
 COL_MAXITER = 2

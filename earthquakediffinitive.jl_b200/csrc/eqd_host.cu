@@ -362,7 +362,6 @@ struct Workspace {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     bool graph_split = false;  // the captured iterations run as two halves
-    uint32_t flags = 0;        // eqd_solve_opts.flags of the batch being recorded
     std::vector<uint64_t> graph_key;  // what the captured graph baked in (see SlotRun::setup)
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1019,8 +1018,7 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, int fused, int k, 
         const cudaGraphNode_t *deps = nullptr;
         size_t ndeps = 0;
         cudaGraphConditionalHandle h;
-        bool cond = !(W.flags & EQD_FLAG_UNGATED) &&
-                    cudaStreamGetCaptureInfo(sn.s, &cst, nullptr, &graph, &deps, &ndeps) == cudaSuccess &&
+        bool cond = cudaStreamGetCaptureInfo(sn.s, &cst, nullptr, &graph, &deps, &ndeps) == cudaSuccess &&
                     cst == cudaStreamCaptureStatusActive &&
                     cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault) == cudaSuccess;
         if (!cond) {
@@ -1256,9 +1254,7 @@ struct SlotRun {
         // workspace pointer (a buffer that grew or was released since the
         // capture must not be reached through the old graph).
         std::vector<uint64_t> kv = {(uint64_t)cap, (uint64_t)o.precision, (uint64_t)generic, (uint64_t)G->sel32,
-                                    (uint64_t)o.precond, (uint64_t)split, (uint64_t)sp.itmax, (uint64_t)fused,
-                                    (uint64_t)(o.flags & EQD_FLAG_UNGATED)};
-        w.flags = o.flags;
+                                    (uint64_t)o.precond, (uint64_t)split, (uint64_t)sp.itmax, (uint64_t)fused};
         for (double d : {sp.rtol, sp.atol, sp.delta}) {
             uint64_t b;
             std::memcpy(&b, &d, sizeof(b));
@@ -1395,8 +1391,7 @@ struct SlotRun {
             // apply, update, scalars, direction (+ the reliable-update condition
             // for mixed precision); the conditional reliable-update kernels are
             // counted from the device counter when the batch ends
-            launches += (int64_t)kIter * ((mixed ? ((w.flags & EQD_FLAG_UNGATED) ? 7 : 5) : 4) - (fused ? 1 : 0)) *
-                        (w.graph_split ? 2 : 1);
+            launches += (int64_t)kIter * ((mixed ? 5 : 4) - (fused ? 1 : 0)) * (w.graph_split ? 2 : 1);
         }
         CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), w.status.p, cap, cudaMemcpyDeviceToHost, G->stream));
         CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), w.iters.p, sizeof(int) * cap, cudaMemcpyDeviceToHost, G->stream));

@@ -29,7 +29,6 @@ end
 # SolveOpts.flags bits (include/eqd.h)
 const EQD_FLAG_STRICT = UInt32(1)    # return an error if a column did not converge
 const EQD_FLAG_NO_SPLIT = UInt32(2)  # one chain of kernels instead of two overlapping halves
-const EQD_FLAG_UNGATED = UInt32(8)   # reliable-update kernels every iteration, not behind a graph condition
 const EQD_FLAG_FUSE = UInt32(4)      # form the CG direction inside the stencil apply
 
 mutable struct SolveOpts

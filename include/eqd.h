@@ -61,9 +61,6 @@ typedef enum { EQD_PRECOND_NONE = 0, EQD_PRECOND_JACOBI = 1 } eqd_precond;
 #define EQD_FLAG_STRICT 1u    /* return EQD_ERR_NOT_CONVERGED if any column did not converge */
 #define EQD_FLAG_NO_SPLIT 2u  /* run a large batch as one chain of kernels instead of two halves whose
                                  stencil applies alternate (for comparisons; results are identical) */
-#define EQD_FLAG_UNGATED 8u   /* mixed precision: launch the reliable-update kernels (fold, FP64 residual,
-                                 scalars) every iteration instead of behind a conditional graph node that
-                                 runs them only when a column is flagged; results are identical */
 #define EQD_FLAG_FUSE 4u      /* form the CG direction p = r + beta p inside the stencil apply (from bulk
                                  copies of r and the previous p) instead of in its own kernel; results
                                  are identical. Off by default: the apply is instruction-issue bound,
