@@ -357,7 +357,6 @@ struct Workspace {
     DevBuf kout;
     DevBuf newmask, slot_list, dst_list;  // slot engine: entering columns, extraction lists
     DevBuf hbuf;                          // explicit-RHS staging (reference layout)
-    DevBuf relcount;                      // reliable-update bodies executed (conditional graph nodes)
     PinnedArr<double> kstage;             // finished K columns on their way to a host K
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
@@ -391,7 +390,6 @@ struct eqd_grid {
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;          // second half of a split batch (graph capture only)
     cudaStream_t stream_hi = nullptr, stream2_hi = nullptr;  // high priority: vector kernels of the halves
-    cudaStream_t stream_cap = nullptr;       // captures the bodies of conditional graph nodes
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evA = nullptr, evB = nullptr, evFork = nullptr, evJoin = nullptr, evArest = nullptr,
                 evBrest = nullptr;
@@ -732,7 +730,6 @@ extern "C" int eqd_grid_create(const eqd_grid_desc *d, eqd_grid **out) {
     CUDA_OR_RETURN(cudaDeviceGetAttribute(&G->num_sms, cudaDevAttrMultiProcessorCount, d->device));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream2, cudaStreamNonBlocking));
-    CUDA_OR_RETURN(cudaStreamCreateWithFlags(&G->stream_cap, cudaStreamNonBlocking));
     {
         int least = 0, greatest = 0;
         CUDA_OR_RETURN(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -761,7 +758,7 @@ extern "C" int eqd_grid_destroy(eqd_grid *G) {
     if (G->ev1) cudaEventDestroy(G->ev1);
     for (cudaEvent_t e : {G->evA, G->evB, G->evFork, G->evJoin, G->evArest, G->evBrest})
         if (e) cudaEventDestroy(e);
-    for (cudaStream_t t : {G->stream2, G->stream_hi, G->stream2_hi, G->stream_cap})
+    for (cudaStream_t t : {G->stream2, G->stream_hi, G->stream2_hi})
         if (t) cudaStreamDestroy(t);
     if (G->stream) cudaStreamDestroy(G->stream);
     delete G;
@@ -998,49 +995,16 @@ static void record_rest(eqd_grid *G, Workspace &W, int mixed, int fused, int k, 
     const unsigned sb = (unsigned)((sn.n + 127) / 128);
     cg_scalar_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp, P.apply_part, P.rr_part, sn.n, mixed);
     if (mixed) {
-        // Reliable update (fold, FP64 true residual, its scalars) for the
-        // flagged columns. In most iterations no column is flagged: the three
-        // kernels sit in the body of a conditional graph node that runs only
-        // when reliable_cond_kernel finds a flagged column in this span.
-        auto reliable = [&](cudaStream_t s) {
-            // One CTA per item: an unflagged column's CTAs return at once.
-            fold_correction_kernel<<<(unsigned)items, kVecThreads, 0, s>>>(P.x64, P.d, P.st, sp, sn.n);
-            ColumnSet cf = P.cs;
-            cf.flag = P.st.flag;
-            cf.dinv = dinv64;
-            launch_march<double, float, MODE_RHS>(G, P.x64, (float *)P.r, cf, P.res_part, sn.n, -1, s);
-            SolveParams sp2 = sp;
-            sp2.ntiles = nparts(G->m64);
-            cg_true_residual_kernel<<<sb, 128, 0, s>>>(P.st, sp2, P.res_part, sn.n, 1);
-        };
-        cudaStreamCaptureStatus cst;
-        cudaGraph_t graph = nullptr;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t ndeps = 0;
-        cudaGraphConditionalHandle h;
-        bool cond = cudaStreamGetCaptureInfo(sn.s, &cst, nullptr, &graph, &deps, &ndeps) == cudaSuccess &&
-                    cst == cudaStreamCaptureStatusActive &&
-                    cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault) == cudaSuccess;
-        if (!cond) {
-            cudaGetLastError();
-            reliable(sn.s);
-        } else {
-            reliable_cond_kernel<<<1, 256, 0, sn.s>>>(h, P.st.flag, P.st.status, sn.n,
-                                                       W.relcount.as<unsigned long long>());
-            cudaStreamGetCaptureInfo(sn.s, &cst, nullptr, &graph, &deps, &ndeps);
-            cudaGraphNodeParams np{};
-            np.type = cudaGraphNodeTypeConditional;
-            np.conditional.handle = h;
-            np.conditional.type = cudaGraphCondTypeIf;
-            np.conditional.size = 1;
-            cudaGraphNode_t node;
-            cudaGraphAddNode(&node, graph, deps, ndeps, &np);
-            cudaStreamUpdateCaptureDependencies(sn.s, &node, 1, cudaStreamSetCaptureDependencies);
-            cudaGraph_t body = np.conditional.phGraph_out[0];
-            cudaStreamBeginCaptureToGraph(G->stream_cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
-            reliable(G->stream_cap);
-            cudaStreamEndCapture(G->stream_cap, &body);
-        }
+        // One CTA per item: in most iterations no column is flagged and every
+        // CTA returns at once.
+        fold_correction_kernel<<<(unsigned)items, kVecThreads, 0, sn.s>>>(P.x64, P.d, P.st, sp, sn.n);
+        ColumnSet cf = P.cs;
+        cf.flag = P.st.flag;
+        cf.dinv = dinv64;
+        launch_march<double, float, MODE_RHS>(G, P.x64, (float *)P.r, cf, P.res_part, sn.n, -1, sn.s);
+        SolveParams sp2 = sp;
+        sp2.ntiles = nparts(G->m64);
+        cg_true_residual_kernel<<<sb, 128, 0, sn.s>>>(P.st, sp2, P.res_part, sn.n, 1);
     }
     if (!fused) {
         const T *dinvT = (const T *)(sizeof(T) == 4 ? (const void *)dinv32 : (const void *)dinv64);
@@ -1206,8 +1170,6 @@ struct SlotRun {
         CUDA_OR_RETURN(w.newmask.ensure(cap));
         CUDA_OR_RETURN(w.slot_list.ensure(sizeof(int) * cap));
         CUDA_OR_RETURN(w.dst_list.ensure(sizeof(int) * cap));
-        CUDA_OR_RETURN(w.relcount.ensure(sizeof(unsigned long long)));
-        CUDA_OR_RETURN(cudaMemsetAsync(w.relcount.p, 0, sizeof(unsigned long long), G->stream));
         CUDA_OR_RETURN(w.slip_node.ensure(sizeof(int) * cap));
         CUDA_OR_RETURN(w.slip_comp.ensure(sizeof(int) * cap));
         if (dense) CUDA_OR_RETURN(w.slip_dense.ensure(sizeof(double) * 2 * gc.nf * cap));
@@ -1262,7 +1224,7 @@ struct SlotRun {
         }
         for (const void *q : {w.x64.p, w.v0.p, w.v1.p, w.v2.p, w.v3.p, w.v4.p, w.apply_part.p, w.res_part.p, w.rr_part.p,
                               w.gamma.p, w.beta.p, w.rr_ref.p, w.tol.p, w.bnorm.p, w.iters.p, w.status.p, w.flag.p,
-                              w.slip_node.p, w.slip_comp.p, w.slip_dense.p, G->dinv64.p, G->dinv32.p, w.relcount.p})
+                              w.slip_node.p, w.slip_comp.p, w.slip_dense.p, G->dinv64.p, G->dinv32.p})
             kv.push_back((uint64_t)(uintptr_t)q);
         if (!w.graph || w.graph_key != kv) {
             if (w.graph) cudaGraphExecDestroy(w.graph);
@@ -1388,10 +1350,7 @@ struct SlotRun {
         for (int s = 0; s < cap; ++s) running += tag[s] >= 0 && hst[s] == COL_ACTIVE;
         if (running > 0) {
             CUDA_OR_RETURN(cudaGraphLaunch(w.graph, G->stream));
-            // apply, update, scalars, direction (+ the reliable-update condition
-            // for mixed precision); the conditional reliable-update kernels are
-            // counted from the device counter when the batch ends
-            launches += (int64_t)kIter * ((mixed ? 5 : 4) - (fused ? 1 : 0)) * (w.graph_split ? 2 : 1);
+            launches += (int64_t)kIter * ((mixed ? 7 : 4) - (fused ? 1 : 0)) * (w.graph_split ? 2 : 1);
         }
         CUDA_OR_RETURN(cudaMemcpyAsync(hst.data(), w.status.p, cap, cudaMemcpyDeviceToHost, G->stream));
         CUDA_OR_RETURN(cudaMemcpyAsync(hit.data(), w.iters.p, sizeof(int) * cap, cudaMemcpyDeviceToHost, G->stream));
@@ -1624,12 +1583,6 @@ static int run_batch(eqd_grid *G, const eqd_solve_opts &o, const BatchSpec &B, e
     if (rc) return rc;
     CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
     CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
-    if (R.mixed) {
-        // Reliable-update bodies that ran (three kernels each).
-        unsigned long long nrel = 0;
-        CUDA_OR_RETURN(cudaMemcpy(&nrel, R.W->relcount.p, sizeof(nrel), cudaMemcpyDeviceToHost));
-        R.launches += 3 * (int64_t)nrel;
-    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, G->ev0, G->ev1);
     if (stats) {

@@ -404,22 +404,6 @@ __global__ void __launch_bounds__(128, 16) cg_pupdate_bulk_kernel(T *__restrict_
     }
 }
 
-// Mixed precision: whether any column of a span is flagged for a reliable
-// update this iteration. Sets the graph condition that gates the update's
-// kernels (fold, FP64 residual apply, true-residual scalars) and counts the
-// iterations that run them. One CTA.
-__global__ void __launch_bounds__(256) reliable_cond_kernel(cudaGraphConditionalHandle h, const int8_t *__restrict__ flag,
-                                                            const int8_t *__restrict__ status, int ncols,
-                                                            unsigned long long *__restrict__ count) {
-    int any = 0;
-    for (int c = threadIdx.x; c < ncols; c += blockDim.x) any |= (status[c] == COL_ACTIVE && flag[c]) ? 1 : 0;
-    any = __syncthreads_or(any);
-    if (threadIdx.x == 0) {
-        cudaGraphSetConditional(h, any ? 1u : 0u);
-        if (any) atomicAdd(count, 1ull);
-    }
-}
-
 // Mixed precision: fold the FP32 correction into the FP64 solution.
 __global__ void __launch_bounds__(256) fold_correction_kernel(double *__restrict__ x, float *__restrict__ d, ColState st,
                                                               SolveParams sp, int ncols) {
