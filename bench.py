@@ -522,6 +522,18 @@ def main():
     batched64_v = len(bcols) / st64.device_seconds
     b64.close()
 
+    # Sparse A of the workload's grid assembled on the GPU (the reference
+    # assembles it with sparse Kronecker algebra before every solve).
+    assembly = None
+    if world == 1:
+        fa = eqd.FaultElasticity(g, lam, MU, lf, device=local)
+        t0 = time.perf_counter()
+        Asp = eqd.assemble_operator(fa, "A")
+        assembly = {"which": "A", "rows": int(Asp.shape[0]), "nnz": int(Asp.nnz),
+                    "seconds": time.perf_counter() - t0, "what": "eqd_assemble to a host CSR (coloured probing)"}
+        del Asp
+        fa.close()
+
     serving = None
     if world == 1 and args.serve_requests > 0:
         serving = serving_leg(eqd, local, args.serve_requests, args.serve_rate)
@@ -572,6 +584,8 @@ def main():
     }
     if serving:
         line["serving"] = serving
+    if assembly:
+        line["assembly"] = assembly
     if gemv:
         line["gemv"] = gemv
     if gemm:

@@ -40,7 +40,7 @@ __all__ = [
     "GridPair", "bp8_grids", "cube_grids", "lame_lambda", "FaultElasticity", "CGSolver",
     "CGStats", "split_node_solve", "solver_report", "merge_stats", "duplicate",
     "elastic_solver_report", "frictional_node_count", "fault_grid_axes", "shear_traction",
-    "fault_stiffness", "fault_stiffness_toeplitz", "stiffness_columns", "apply_operator",
+    "fault_stiffness", "fault_stiffness_toeplitz", "stiffness_columns", "apply_operator", "assemble_operator",
     "KMatrix", "build_model", "EqdError", "EqdArgumentError", "library_path", "Server",
     "operator_diagonal", "jacobi_preconditioner", "cached_fault_stiffness", "BP8Rhs", "FrictionParams",
     "friction_solve",
@@ -339,6 +339,26 @@ def apply_operator(fe, x, mode="A", precision="fp64"):
     check(lib().eqd_apply(fe.handle, ptr(X), ptr(Y), C.c_int32(X.shape[0]), C.c_int32(m),
                           C.c_int32(_PRECISIONS[precision])))
     return Y[0].copy() if one else Y.T.copy()
+
+
+def assemble_operator(fe, which="A"):
+    """The assembled sparse matrix of `split_node_system`
+    (src/ElasticitySplitNode.jl:106-214): "A" = -H P (D+SAT) P or "HP_DSAT"
+    = H P (D+SAT), as a scipy CSR matrix in the reference DOF order, built on
+    the GPU by coloured probing of the matrix-free operator. Entries below
+    1e-12 of their row's largest are left out (numerically zero)."""
+    import scipy.sparse as sp
+    w = {"A": 0, "HP_DSAT": 1}[which]
+    nnz = C.c_int64()
+    check(lib().eqd_assemble(fe.handle, C.c_int32(w), C.c_int64(0), None, None, None, C.byref(nnz)))
+    n = fe.Ntot
+    indptr = np.empty(n + 1, dtype=np.int64)
+    indices = np.empty(max(nnz.value, 1), dtype=np.int32)
+    values = np.empty(max(nnz.value, 1))
+    check(lib().eqd_assemble(fe.handle, C.c_int32(w), C.c_int64(len(values)), ptr(indptr), ptr(indices),
+                             ptr(values), C.byref(nnz)))
+    k = nnz.value
+    return sp.csr_matrix((values[:k], indices[:k], indptr), shape=(n, n))
 
 
 def shear_traction(fe, s2, s3, solver=None):

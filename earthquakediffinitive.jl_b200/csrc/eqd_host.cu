@@ -1860,6 +1860,109 @@ extern "C" int eqd_test_inject_wait_timeout(eqd_grid *G, int32_t plane, uint32_t
     return EQD_OK;
 }
 
+// Sparse A (which = 0) or HP_DSAT (which = 1) in reference DOF order, CSR,
+// by coloured probing with the FP64 operator kernels (probe_* kernels).
+static constexpr int kProbeRowCap = 128;        // entries a row may hold before the drop (measured at most 96)
+static constexpr double kProbeRelDrop = 1e-12;  // entries below this fraction of the row's largest are rounding
+
+extern "C" int eqd_assemble(eqd_grid *G, int32_t which, int64_t capacity, int64_t *indptr, int32_t *indices,
+                            double *values, int64_t *nnz) {
+    if (!G || !nnz || (which != 0 && which != 1) || capacity < 0) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    const GridConst &gc = G->gc;
+    ProbeGeom pg{};
+    pg.n1 = gc.n1;
+    pg.n2 = gc.n2;
+    pg.n3 = gc.n3;
+    pg.PS = gc.PS;
+    pg.colstride = gc.colstride;
+    pg.N = (long long)gc.n1 * gc.n2 * gc.n3;
+    pg.R = 6;
+    pg.P2 = gc.n2 <= 2 * pg.R + 1 ? gc.n2 : 2 * pg.R + 1;
+    pg.P3 = gc.n3 <= 2 * pg.R + 1 ? gc.n3 : 2 * pg.R + 1;
+    pg.ncolors = 6LL * gc.n1 * pg.P2 * pg.P3;
+    const long long ntot = 6 * pg.N;
+    if (ntot > INT32_MAX) return fail(EQD_ERR_UNSUPPORTED, "more DOFs than 32-bit column indices hold");
+    // Probe chunk: at most 512 colours, within a quarter of free memory for x and y.
+    size_t fr = 0, tot = 0;
+    CUDA_OR_RETURN(cudaMemGetInfo(&fr, &tot));
+    const size_t per = 2 * sizeof(double) * (size_t)gc.colstride;
+    long long nc = std::min<long long>({512, pg.ncolors, (long long)(fr / 4 / per)});
+    if (nc < 1) return fail(EQD_ERR_OOM, "no room for one probe");
+    DevBuf x, y, sn, scomp, rcnt, rcol, rval, rmax, kept, dptr, dind, dval, ovf;
+    CUDA_OR_RETURN(x.ensure(sizeof(double) * gc.colstride * nc));
+    CUDA_OR_RETURN(y.ensure(sizeof(double) * gc.colstride * nc));
+    CUDA_OR_RETURN(sn.ensure(sizeof(int) * nc));
+    CUDA_OR_RETURN(scomp.ensure(sizeof(int) * nc));
+    CUDA_OR_RETURN(rcnt.ensure(sizeof(int) * ntot));
+    CUDA_OR_RETURN(rcol.ensure(sizeof(int) * ntot * kProbeRowCap));
+    CUDA_OR_RETURN(rval.ensure(sizeof(double) * ntot * kProbeRowCap));
+    CUDA_OR_RETURN(rmax.ensure(sizeof(double) * ntot));
+    CUDA_OR_RETURN(kept.ensure(sizeof(long long) * ntot));
+    CUDA_OR_RETURN(ovf.ensure(sizeof(unsigned)));
+    cudaStream_t st = G->stream;
+    CUDA_OR_RETURN(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * ntot, st));
+    CUDA_OR_RETURN(cudaMemsetAsync(rmax.p, 0, sizeof(double) * ntot, st));
+    CUDA_OR_RETURN(cudaMemsetAsync(ovf.p, 0, sizeof(unsigned), st));
+    {
+        std::vector<int> neg(nc, -1);
+        CUDA_OR_RETURN(cudaMemcpyAsync(sn.p, neg.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+        CUDA_OR_RETURN(cudaMemsetAsync(scomp.p, 0, sizeof(int) * nc, st));
+        CUDA_OR_RETURN(cudaStreamSynchronize(st));
+    }
+    ColumnSet cs{};
+    cs.slip_node = sn.as<int>();  // no slip: HP_DSAT x without the chi term
+    cs.slip_comp = scomp.as<int>();
+    const unsigned rb = (unsigned)((ntot + 255) / 256);
+    for (long long c0 = 0; c0 < pg.ncolors; c0 += nc) {
+        const int n = (int)std::min<long long>(nc, pg.ncolors - c0);
+        CUDA_OR_RETURN(cudaMemsetAsync(x.p, 0, sizeof(double) * gc.colstride * n, st));
+        probe_fill_kernel<<<1184, 256, 0, st>>>(pg, c0, n, x.as<double>());
+        CUDA_OR_RETURN(cudaGetLastError());
+        if (which == 0)
+            CUDA_OR_RETURN((launch_march<double, double, MODE_AP>(G, x.as<double>(), y.as<double>(), cs, nullptr, n)));
+        else
+            CUDA_OR_RETURN((launch_march<double, double, MODE_RHS>(G, x.as<double>(), y.as<double>(), cs, nullptr, n)));
+        probe_extract_kernel<<<rb, 256, 0, st>>>(pg, c0, n, y.as<double>(), kProbeRowCap, rcnt.as<int>(), rcol.as<int>(),
+                                                 rval.as<double>(), rmax.as<double>(), ovf.as<unsigned>());
+        CUDA_OR_RETURN(cudaGetLastError());
+    }
+    probe_compact_kernel<<<rb, 256, 0, st>>>(ntot, kProbeRowCap, rcnt.as<int>(), rcol.as<int>(), rval.as<double>(),
+                                             rmax.as<double>(), kProbeRelDrop, 0, nullptr, nullptr, nullptr,
+                                             kept.as<long long>());
+    CUDA_OR_RETURN(cudaGetLastError());
+    std::vector<long long> cnt(ntot);
+    unsigned hovf = 0;
+    CUDA_OR_RETURN(cudaMemcpyAsync(cnt.data(), kept.p, sizeof(long long) * ntot, cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaMemcpyAsync(&hovf, ovf.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaStreamSynchronize(st));
+    int rc = check_device_error(G);
+    if (rc) return rc;
+    if (hovf) return fail(EQD_ERR_UNSUPPORTED, "a row holds more than " + std::to_string(kProbeRowCap) + " entries");
+    std::vector<long long> off(ntot + 1, 0);
+    for (long long i = 0; i < ntot; ++i) off[i + 1] = off[i] + cnt[i];
+    *nnz = off[ntot];
+    if (!indptr && !indices && !values) return EQD_OK;  // size query
+    if (!indptr || !indices || !values) return fail(EQD_ERR_ARG, "indptr, indices and values go together");
+    if (capacity < off[ntot])
+        return fail(EQD_ERR_ARG, "capacity " + std::to_string(capacity) + " below nnz " + std::to_string(off[ntot]));
+    CUDA_OR_RETURN(dptr.ensure(sizeof(long long) * (ntot + 1)));
+    CUDA_OR_RETURN(dind.ensure(sizeof(int) * std::max<long long>(off[ntot], 1)));
+    CUDA_OR_RETURN(dval.ensure(sizeof(double) * std::max<long long>(off[ntot], 1)));
+    CUDA_OR_RETURN(cudaMemcpyAsync(dptr.p, off.data(), sizeof(long long) * (ntot + 1), cudaMemcpyHostToDevice, st));
+    probe_compact_kernel<<<rb, 256, 0, st>>>(ntot, kProbeRowCap, rcnt.as<int>(), rcol.as<int>(), rval.as<double>(),
+                                             rmax.as<double>(), kProbeRelDrop, 1, dptr.as<long long>(), dind.as<int>(),
+                                             dval.as<double>(), nullptr);
+    CUDA_OR_RETURN(cudaGetLastError());
+    CUDA_OR_RETURN(cudaMemcpyAsync(indices, dind.p, sizeof(int) * off[ntot], cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaMemcpyAsync(values, dval.p, sizeof(double) * off[ntot], cudaMemcpyDeviceToHost, st));
+    CUDA_OR_RETURN(cudaStreamSynchronize(st));
+    for (long long i = 0; i <= ntot; ++i) indptr[i] = off[i];
+    return EQD_OK;
+}
+
 extern "C" int eqd_diag(eqd_grid *G, double *d) {
     if (!G || !d) return fail(EQD_ERR_ARG, "invalid argument");
     std::lock_guard<std::mutex> lk(G->mtx);

@@ -925,6 +925,138 @@ __global__ void gemv_reduce_kernel(const double *__restrict__ part, long long n,
     y[gid] = s;
 }
 
+// ---------------------------------------------------------------------------
+// Sparse assembly of A or HP_DSAT by coloured probing (`split_node_system`,
+// src/ElasticitySplitNode.jl:106-214, for callers that want the matrices).
+// A DOF j of block sc (side * 3 + comp) at point (j1, j2, j3) has colour
+//   ((sc * n1 + j1) * P2 + j2 mod P2) * P3 + j3 mod P3,
+// with P = n on short axes and P = 2 R + 1 otherwise, R = the largest
+// index distance between a row and a column of a nonzero along x2 and x3
+// (measured: 5; R = 6 is used). Applying the operator to the indicator of
+// one colour gives, in row i, the entry A[i, j] of the only column j of
+// that colour within R of i along x2 and x3 (every colour-mate of j lies
+// further away, where A[i, .] is zero).
+// ---------------------------------------------------------------------------
+struct ProbeGeom {
+    int n1, n2, n3, PS;
+    long long colstride, N;   // N = n1 n2 n3 points per block
+    int P2, P3, R;
+    long long ncolors;
+};
+
+__host__ __device__ inline long long probe_color(const ProbeGeom &g, int sc, int j1, int j2, int j3) {
+    return (((long long)sc * g.n1 + j1) * g.P2 + j2 % g.P2) * g.P3 + j3 % g.P3;
+}
+
+// Indicators of colours [c0, c0 + nc), device layout, FP64.
+__global__ void probe_fill_kernel(ProbeGeom g, long long c0, int nc, double *__restrict__ x) {
+    const long long ntot = 6 * g.N;
+    for (long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x; gid < ntot;
+         gid += (long long)gridDim.x * blockDim.x) {
+        const int sc = (int)(gid / g.N);
+        const long long pt = gid % g.N;
+        const int i3 = (int)(pt / ((long long)g.n1 * g.n2));
+        const int i2 = (int)((pt / g.n1) % g.n2);
+        const int i1 = (int)(pt % g.n1);
+        const long long c = probe_color(g, sc, i1, i2, i3) - c0;
+        if (c >= 0 && c < nc) x[c * g.colstride + ((long long)sc * g.n3 + i3) * g.PS + (long long)i2 * g.n1 + i1] = 1.0;
+    }
+}
+
+// The column of colour c near row position (i2, i3): its reference index,
+// or -1 when that colour has no column within R of the row along x2 / x3.
+__device__ __forceinline__ long long probe_column(const ProbeGeom &g, long long c, int i2, int i3) {
+    const int r3 = (int)(c % g.P3);
+    const int r2 = (int)((c / g.P3) % g.P2);
+    const int j1 = (int)((c / ((long long)g.P3 * g.P2)) % g.n1);
+    const int sc = (int)(c / ((long long)g.P3 * g.P2 * g.n1));
+    auto near_ = [&](int i, int r, int P, int n) -> int {
+        if (P == n) return r;  // short axis: every index has its own colour
+        const int lo = i - g.R;
+        const int j = lo + (((r - lo) % P) + P) % P;
+        return (j >= 0 && j < n) ? j : -1;
+    };
+    const int j2 = near_(i2, r2, g.P2, g.n2);
+    const int j3 = near_(i3, r3, g.P3, g.n3);
+    if (j2 < 0 || j3 < 0) return -1;
+    return (long long)sc * g.N + ((long long)j3 * g.n2 + j2) * g.n1 + j1;
+}
+
+// Row i (reference order) takes, for each colour of the chunk, the entry the
+// probe produced in that row, into a per-row buffer of kcap (column, value)
+// pairs; rowmax tracks the largest magnitude of the row.
+__global__ void probe_extract_kernel(ProbeGeom g, long long c0, int nc, const double *__restrict__ y, int kcap,
+                                     int *__restrict__ rcnt, int *__restrict__ rcol, double *__restrict__ rval,
+                                     double *__restrict__ rmax, unsigned *__restrict__ overflow) {
+    const long long ntot = 6 * g.N;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntot) return;
+    const int sc = (int)(i / g.N);
+    const long long pt = i % g.N;
+    const int i3 = (int)(pt / ((long long)g.n1 * g.n2));
+    const int i2 = (int)((pt / g.n1) % g.n2);
+    const long long dev = ((long long)sc * g.n3 + i3) * g.PS + (pt % ((long long)g.n1 * g.n2));
+    int cnt = rcnt[i];
+    double mx = rmax[i];
+    for (int k = 0; k < nc; ++k) {
+        const long long j = probe_column(g, c0 + k, i2, i3);
+        if (j < 0) continue;
+        const double v = y[(long long)k * g.colstride + dev];
+        if (v == 0.0) continue;
+        if (cnt < kcap) {
+            rcol[i * kcap + cnt] = (int)j;
+            rval[i * kcap + cnt] = v;
+        } else {
+            atomicOr(overflow, 1u);
+        }
+        ++cnt;
+        mx = fmax(mx, fabs(v));
+    }
+    rcnt[i] = cnt;
+    rmax[i] = mx;
+}
+
+// Per row: sort the buffered entries by column and drop those below
+// rel_drop times the row's largest (rounding residue of exactly cancelling
+// terms); pass 0 writes the kept count, pass 1 the CSR entries at offset
+// indptr[i].
+__global__ void probe_compact_kernel(long long ntot, int kcap, int *__restrict__ rcnt, int *__restrict__ rcol,
+                                     double *__restrict__ rval, const double *__restrict__ rmax, double rel_drop,
+                                     int pass, const long long *__restrict__ indptr, int *__restrict__ indices,
+                                     double *__restrict__ values, long long *__restrict__ kept) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntot) return;
+    const int n = min(rcnt[i], kcap);
+    int *cols = rcol + i * kcap;
+    double *vals = rval + i * kcap;
+    if (pass == 0) {
+        for (int a = 1; a < n; ++a) {  // insertion sort by column
+            const int cj = cols[a];
+            const double vj = vals[a];
+            int b = a - 1;
+            while (b >= 0 && cols[b] > cj) {
+                cols[b + 1] = cols[b];
+                vals[b + 1] = vals[b];
+                --b;
+            }
+            cols[b + 1] = cj;
+            vals[b + 1] = vj;
+        }
+    }
+    const double thr = rel_drop * rmax[i];
+    long long o = pass == 1 ? indptr[i] : 0;
+    long long m = 0;
+    for (int a = 0; a < n; ++a) {
+        if (fabs(vals[a]) <= thr) continue;
+        if (pass == 1) {
+            indices[o + m] = cols[a];
+            values[o + m] = vals[a];
+        }
+        ++m;
+    }
+    if (pass == 0) kept[i] = m;
+}
+
 // Deterministic pseudo-random fill in [-1, 1) (measurement inputs).
 template <typename T>
 __global__ void fill_random_kernel(T *__restrict__ v, long long n, unsigned long long seed) {

@@ -206,6 +206,19 @@ int eqd_set_variant(eqd_grid *grid, int32_t variant);
  * EQD_ERR_TIMEOUT; later calls run normally. One launch only. */
 int eqd_test_inject_wait_timeout(eqd_grid *grid, int32_t plane, uint32_t poll_limit);
 
+/* The assembled matrices of `split_node_system` (src/ElasticitySplitNode.jl:
+ * 106-214) for callers that want them: which = 0 gives A = -H P (D+SAT) P,
+ * which = 1 gives HP_DSAT = H P (D+SAT), CSR in reference DOF order (ntot
+ * rows, 0-based, columns ascending), built on the GPU by coloured probing with
+ * the FP64 operator kernels (no Julia-side assembly). Holds the numerically
+ * nonzero entries: entries below 1e-12 of their row's largest (the rounding
+ * of exactly cancelling terms, and the explicit zeros of the reference's
+ * structural pattern) are left out. With indptr, indices and values all NULL
+ * only *nnz is set; otherwise indptr holds ntot + 1 entries and indices and
+ * values `capacity` >= *nnz entries (EQD_ERR_ARG with *nnz set when smaller). */
+int eqd_assemble(eqd_grid *grid, int32_t which, int64_t capacity, int64_t *indptr, int32_t *indices,
+                 double *values, int64_t *nnz);
+
 /* Jacobi diagonal, `diag(A)` (src/ElasticitySplitNode.jl:352-357), reference layout. */
 int eqd_diag(eqd_grid *grid, double *d);
 
