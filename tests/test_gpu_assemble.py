@@ -8,12 +8,13 @@ from oracle.operators import Grid3, SplitNodeSystem
 
 pytestmark = pytest.mark.gpu
 
-# (n1, n2, n3, x1_extent, x2 range, x3 range, lam, mu)
+# (n1, n2, n3, x1_extent, x2 range, x3 range, lam, mu, l_f); l_f only selects
+# Omega_f (it does not enter the matrices) and must land on grid nodes
 CASES = [
-    (11, 11, 11, 1.0, (-1, 1), (-1, 1), 2.0, 1.0),                  # the reference's test cubes
-    (9, 17, 21, 0.8, (-1.6, 1.6), (-2.0, 2.0), 1.5, 0.7),           # unequal spacings, periodic colours on x2, x3
-    (12, 10, 9, 1.0, (-1, 1), (-1, 1), 2.0, 1.0),                   # even / shortest axes
-    (9, 17, 17, 800.0, (-800, 800), (-800, 800), 32.04e9, 32.04e9), # BP8 units, h = 100 m
+    (11, 11, 11, 1.0, (-1, 1), (-1, 1), 2.0, 1.0, 0.4),                  # the reference's test cubes
+    (9, 17, 21, 0.8, (-1.6, 1.6), (-2.0, 2.0), 1.5, 0.7, 0.0),           # unequal spacings, periodic colours
+    (12, 10, 9, 1.0, (-1, 1), (-1, 1), 2.0, 1.0, 1.0),                   # even / shortest axes
+    (9, 17, 17, 800.0, (-800, 800), (-800, 800), 32.04e9, 32.04e9, 400.0),  # BP8 units, h = 100 m
 ]
 
 
@@ -31,12 +32,12 @@ def kept(M, rel):
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}")
 @pytest.mark.parametrize("which", ["A", "HP_DSAT"])
 def test_assembly_matches_oracle(eqd, case, which):
-    n1, n2, n3, L1, x2, x3, lam, mu = case
+    n1, n2, n3, L1, x2, x3, lam, mu, l_f = case
     gm = Grid3((-L1, x2[0], x3[0]), (0.0, x2[1], x3[1]), (n1, n2, n3))
     gp = Grid3((0.0, x2[0], x3[0]), (L1, x2[1], x3[1]), (n1, n2, n3))
     S = SplitNodeSystem(gm, gp, lam, mu)
     ref = S.A if which == "A" else S.HP_DSAT
-    fe = eqd.FaultElasticity(eqd.GridPair(n1, n2, n3, L1, x2, x3), lam, mu, 0.0)
+    fe = eqd.FaultElasticity(eqd.GridPair(n1, n2, n3, L1, x2, x3), lam, mu, l_f)
     M = eqd.assemble_operator(fe, which)
     assert M.shape == ref.shape
     R, rmax = kept(ref, 1e-10)
