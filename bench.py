@@ -398,6 +398,11 @@ def main():
                 "variants": [{"tile_rows": trows[i], "threads": tthr[i], "ms_per_cg_iteration": tms[i]}
                              for i in range(nv.value)]}
     kernel = apply_kernel_name(sel.value, n1, trows[sel.value], tthr[sel.value])
+    # Chunk-width tuner (after the timed steps, which ran at the budget's width).
+    widths = [w for w in (32, 64, 128, 256, 512, 1024, 2048, 4096) if w <= len(cols)]
+    cbest, ctable = eqd.tune_chunk(fe, widths)
+    chunk_tuning = {"best": cbest, "ms_per_column_iteration": {str(w): m for w, m in ctable},
+                    "timed_steps_width": "HBM budget (100 GiB at h = 20 m and 25 m, else free memory)"}
 
     # Roofline of the dominant kernel: FP32 stencil apply over the batch.
     ms = C.c_double()
@@ -577,6 +582,7 @@ def main():
                      "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                      "peak_kind": peak_kind, "columns_per_launch": napply},
         "autotune": autotune,
+        "chunk_tuning": chunk_tuning,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -267,6 +267,17 @@ def autotune(fe, ncols=256):
     return sel.value, [(tr[i], tt[i], ms[i]) for i in range(nv.value)]
 
 
+def tune_chunk(fe, widths=(32, 64, 128, 256, 512, 1024)):
+    """Time mixed-precision CG iterations at each batch width; returns (best
+    width, [(width, ms per column-iteration or None when out of range)]).
+    Later calls on this grid with chunk=0 use the best width."""
+    w = np.ascontiguousarray(widths, dtype=np.int32)
+    ms = np.empty(len(w))
+    best = C.c_int32()
+    check(lib().eqd_tune_chunk(fe.handle, ptr(w), C.c_int32(len(w)), ptr(ms), C.byref(best)))
+    return best.value, [(int(a), (float(b) if b >= 0 else None)) for a, b in zip(w, ms)]
+
+
 def frictional_node_count(fe):
     return fe.nf
 

@@ -385,6 +385,7 @@ struct eqd_grid {
     int v32_lanes[kNumVariants] = {};
     int sel32 = 0;
     bool tuned = false;
+    int chunk_tuned = 0;   // eqd_tune_chunk's choice of columns per batch (0: as many as the budget allows)
     double tune_ms[kNumVariants] = {};
     int nchunks = 1;
     cudaStream_t stream = nullptr;
@@ -877,7 +878,9 @@ static int resolve_chunk(eqd_grid *G, const eqd_solve_opts &o, int ncols, int pr
     }
     long long cap = (long long)(budget / per_col);
     if (cap < 1) return fail(EQD_ERR_OOM, "HBM budget too small for one column");
-    chunk = o.chunk > 0 ? std::min(o.chunk, ncols) : (int)std::min<long long>(cap, ncols);
+    const long long want =
+        o.chunk > 0 ? o.chunk : ((G->chunk_tuned > 0 && prec == EQD_PREC_MIXED) ? G->chunk_tuned : cap);
+    chunk = (int)std::min<long long>(want, ncols);
     if ((long long)chunk > cap) chunk = (int)cap;
     return EQD_OK;
 }
@@ -1838,6 +1841,64 @@ extern "C" int eqd_autotune(eqd_grid *G, int32_t ncols, int32_t *selected, doubl
         if (threads) threads[v] = G->v32[v].threads;
     }
     return EQD_OK;
+}
+
+// Chunk-width tuner: the cost of one column-iteration of the mixed-precision
+// CG at each batch width (unit-slip columns, two graph launches = 20
+// iterations after one untimed launch), and the cheapest width, which later
+// calls with opts.chunk = 0 use (capped by the HBM budget).
+extern "C" int eqd_tune_chunk(eqd_grid *G, const int32_t *widths, int32_t nwidths, double *ms_per_column_iteration,
+                              int32_t *best) {
+    if (!G || !widths || nwidths < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> lk(G->mtx);
+    if (G->served) return fail(EQD_ERR_ARG, "the grid is attached to a server");
+    CUDA_OR_RETURN(cudaSetDevice(G->desc.device));
+    const GridConst &gc = G->gc;
+    eqd_solve_opts o;
+    eqd_default_opts(&o);
+    int cap = 0;
+    int rc = resolve_chunk(G, o, 2 * gc.nf, EQD_PREC_MIXED, cap);
+    if (rc) return rc;
+    double bestms = 1e300;
+    int bestw = 0;
+    for (int k = 0; k < nwidths; ++k) {
+        const int w = widths[k];
+        if (w < 1 || w > 2 * gc.nf || w > cap) {
+            if (ms_per_column_iteration) ms_per_column_iteration[k] = -1.0;  // not measured: out of range
+            continue;
+        }
+        std::vector<ColWork> work(w);
+        for (int i = 0; i < w; ++i) {
+            work[i].slip_node = (int)(((long long)i * 7919 + gc.nf / 2) % gc.nf);
+            work[i].slip_comp = i & 1;
+            work[i].tag = i;
+        }
+        SlotRun<float> R;
+        rc = R.setup(G, o, w, false, false);
+        if (rc) return rc;
+        int taken = 0;
+        rc = R.admit(work.data(), w, taken);
+        if (!rc) rc = R.launch();
+        if (rc) return rc;
+        CUDA_OR_RETURN(cudaEventRecord(G->ev0, G->stream));
+        rc = R.launch();
+        if (!rc) rc = R.launch();
+        if (rc) return rc;
+        CUDA_OR_RETURN(cudaEventRecord(G->ev1, G->stream));
+        CUDA_OR_RETURN(cudaEventSynchronize(G->ev1));
+        float ms = 0.f;
+        CUDA_OR_RETURN(cudaEventElapsedTime(&ms, G->ev0, G->ev1));
+        const double per = ms / (2.0 * SlotRun<float>::kIter * w);
+        if (ms_per_column_iteration) ms_per_column_iteration[k] = per;
+        if (per < bestms) {
+            bestms = per;
+            bestw = w;
+        }
+    }
+    if (bestw == 0) return fail(EQD_ERR_ARG, "no width within 1 .. min(2 nf, the budget's columns)");
+    G->chunk_tuned = bestw;
+    if (best) *best = bestw;
+    return check_device_error(G);
 }
 
 extern "C" int eqd_set_variant(eqd_grid *G, int32_t variant) {

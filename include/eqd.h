@@ -94,7 +94,8 @@ typedef struct {
     int64_t itmax;            /* 0 -> 2 Ntot, Krylov's default */
     int32_t precond;          /* eqd_precond */
     int32_t precision;        /* eqd_precision */
-    int32_t chunk;            /* columns per device batch; 0 -> as many as the HBM budget allows */
+    int32_t chunk;            /* columns per device batch; 0 -> eqd_tune_chunk's choice if the grid was
+                                 tuned, else as many as the HBM budget allows */
     double reliable_delta;    /* mixed: FP64 true-residual update when ||r|| drops by this factor (0 -> 0.01) */
     uint64_t hbm_budget_bytes;/* 0 -> free device memory minus 2 GiB */
     int32_t variant;          /* FP32 stencil launch variant for this call: 0 -> the grid's (chosen by
@@ -193,6 +194,13 @@ int eqd_profile_apply(eqd_grid *grid, int32_t ncols, int32_t precision, int32_t 
  * of the last tuning (zeros if the grid was never tuned). */
 int eqd_autotune(eqd_grid *grid, int32_t ncols, int32_t *selected, double *ms_per_variant, int32_t *tile_rows,
                  int32_t *threads, int32_t *nvariants);
+
+/* Chunk-width tuner (columns per batch): times 20 mixed-precision CG
+ * iterations of `widths[k]` unit-slip columns for each width, writes the cost
+ * of one column-iteration (ms; -1 for a width above 2nf or the HBM budget)
+ * and the cheapest width, which later calls with opts.chunk = 0 use. */
+int eqd_tune_chunk(eqd_grid *grid, const int32_t *widths, int32_t nwidths, double *ms_per_column_iteration,
+                   int32_t *best);
 
 /* Pins the FP32 stencil launch variant (0 .. *nvariants-1 of eqd_autotune)
  * for this grid instead of autotuning (reproducibility across processes). */

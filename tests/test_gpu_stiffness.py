@@ -111,6 +111,19 @@ def _batched_equals_single(eqd, precision, variant):
     assert np.array_equal(Kp[:, ::-1], Kb)
 
 
+def test_tune_chunk(eqd, small):
+    """The chunk-width tuner measures every width within range, skips the
+    rest, and later builds (which then use its width) give the same K bits."""
+    fe = eqd.FaultElasticity(eqd.cube_grids(11), LAM, MU, 0.4)
+    eqd.set_stencil_variant(fe, 1)
+    K0 = eqd.fault_stiffness(fe)
+    best, table = eqd.tune_chunk(fe, (8, 16, 32, 1000))
+    assert [w for w, _ in table] == [8, 16, 32, 1000]
+    assert table[3][1] is None and all(ms > 0 for _, ms in table[:3])
+    assert best in (8, 16, 32)
+    assert np.array_equal(eqd.fault_stiffness(fe), K0)
+
+
 def test_toeplitz(eqd, small):
     """test/fault_response_test.jl:128-171."""
     ofe, K_exact = small
