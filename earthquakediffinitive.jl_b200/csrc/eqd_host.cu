@@ -2089,11 +2089,11 @@ static int gemv_slices(int n) {
 // vectors) instead of the GEMV (K read once per 4 vectors).
 static constexpr int kGemmMinVectors = 8;
 
-// Column slices of the blocked K S: enough CTAs for two per SM, each slice
-// at least 256 columns of K.
+// Column slices of the blocked K S: enough CTAs for eight per SM (their
+// loads and the tile barriers overlap), each slice at least 256 columns of K.
 static int gemm_slices(int n, int nvec) {
     const long long tiles = (long long)((n + kGemmBM - 1) / kGemmBM) * ((nvec + kGemmBN - 1) / kGemmBN);
-    const long long want = (2LL * 148 + tiles - 1) / tiles;
+    const long long want = (8LL * 148 + tiles - 1) / tiles;
     return (int)std::max<long long>(1, std::min<long long>(want, std::max(1, n / 256)));
 }
 

@@ -850,7 +850,9 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // Blocked FP64 K S for many slip vectors (Runge-Kutta stages, ensembles):
 // K is read once per 64 vectors instead of once per 4. CTA tile: 64 rows of
 // K x 64 vectors over the k-range of one column slice, in steps of 16 columns
-// staged in shared memory; each of the 256 threads accumulates a 4 x 4 block
+// staged in shared memory (each thread loads its share of the next step's
+// tiles into registers while the current step is computed); each of the 256
+// threads accumulates a 4 x 4 block
 // (rows ty + 16 i, vectors tx + 16 j) in a fixed k order. Partial sums go to
 // part[(v * nslice + slice) * n + row], the GEMV's layout, and the same
 // fixed-order reduction over slices finishes them.
@@ -867,27 +869,36 @@ __global__ void __launch_bounds__(256) gemm_ks_partial_kernel(const double *__re
     const int slice = blockIdx.y;
     const int v0 = blockIdx.z * kGemmBN;
     const long long c0 = n * slice / nslice, c1 = n * (slice + 1) / nslice;
+    // This thread's share of a K tile (rows r, columns kk + 4 q) and of an S
+    // tile (entries kk2 of vectors j2 + 16 q), held in registers so that the
+    // next tile's loads are in flight while the current tile is used.
+    const int ar = tid % kGemmBM, akk = tid / kGemmBM;
+    const int bkk = tid % kGemmBK, bj = tid / kGemmBK;
+    double ra[4], rb[4];
+    auto load = [&](long long k0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long long row = row0 + ar, c = k0 + akk + 4 * q;
+            ra[q] = (row < n && c < c1) ? K[c * n + row] : 0.0;
+            const long long cb = k0 + bkk;
+            const int j = bj + 16 * q;
+            rb[q] = (cb < c1 && v0 + j < nvec) ? S[(long long)(v0 + j) * n + cb] : 0.0;
+        }
+    };
     double acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    if (c0 < c1) load(c0);
     for (long long k0 = c0; k0 < c1; k0 += kGemmBK) {
-        // K tile: rows row0 .. row0 + 63 (contiguous in a column), 16 columns
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int r = tid % kGemmBM, kk = tid / kGemmBM + 4 * q;
-            const long long row = row0 + r, c = k0 + kk;
-            As[kk][r] = (row < n && c < c1) ? K[c * n + row] : 0.0;
-        }
-        // S tile: 16 consecutive entries of each of 64 vectors
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int kk = tid % kGemmBK, j = tid / kGemmBK + 16 * q;
-            const long long c = k0 + kk;
-            Bs[kk][j] = (c < c1 && v0 + j < nvec) ? S[(long long)(v0 + j) * n + c] : 0.0;
+            As[akk + 4 * q][ar] = ra[q];
+            Bs[bkk][bj + 16 * q] = rb[q];
         }
         __syncthreads();
+        if (k0 + kGemmBK < c1) load(k0 + kGemmBK);
 #pragma unroll
         for (int kk = 0; kk < kGemmBK; ++kk) {
             double a[4], b[4];
