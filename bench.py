@@ -462,12 +462,36 @@ def main():
         for _ in range(reps):
             Ym = KM.gemv(Sm)
         gdt = (time.perf_counter() - t0) / reps
+        # The same product on device-resident slips (eqd_kmat_gemv_device):
+        # the blocked kernel and its slice reduction, timed by CUDA events.
+        sd = torch.from_numpy(np.ascontiguousarray(Sm.T)).to(f"cuda:{local}")
+        yd = torch.empty_like(sd)
+        stream = torch.cuda.current_stream()
+        KM.gemv_device(sd, yd, stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dreps = 10
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(dreps):
+            KM.gemv_device(sd, yd, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dms = e0.elapsed_time(e1) / dreps
+        Ydev = yd.cpu().numpy().T
         KM.close()
         Yref = Kmix @ Sm
+        props = torch.cuda.get_device_properties(local)
+        sm_max = (clocks or {}).get("sm_max_mhz") or 1965.0
+        fp64_peak = props.multi_processor_count * 128 * sm_max * 1e6 / 1e12
+        dtf = 2.0 * n * n * nv / (dms * 1e-3) / 1e12
         gemm = {"n": n, "nvec": nv, "ms": gdt * 1e3, "GFLOP_s": 2.0 * n * n * nv / gdt / 1e9,
                 "K_GB_s": 8.0 * n * n / gdt / 1e9,
                 "rel_err_vs_host": float(np.linalg.norm(Ym - Yref) / np.linalg.norm(Yref)),
-                "what": "eqd_kmat_gemv with 64 vectors through the host API (copies of S and Y included)"}
+                "what": "eqd_kmat_gemv with 64 vectors through the host API (copies of S and Y included)",
+                "device": {"ms": dms, "TFLOP_s": dtf, "peak_TFLOP_s": fp64_peak, "frac": dtf / fp64_peak,
+                           "peak_kind": "nominal FP64 (SMs x 128 flop/clk x max SM clock)",
+                           "same_bits_as_host_api": bool(np.array_equal(Ydev, Ym)),
+                           "what": "eqd_kmat_gemv_device on resident slips, CUDA events, 10 calls"}}
 
     # The Toeplitz mode's 10 source solves (src/FaultResponse.jl:339-393:
     # the centre node, then the four corners, each with s2 and s3) on the

@@ -463,6 +463,25 @@ class KMatrix:
         check(lib().eqd_kmat_gemv(self._h, ptr(S), ptr(Y), C.c_int32(S.shape[0])))
         return Y[0].copy() if one else Y.T.copy()
 
+    def gemv_device(self, s, y, stream=None):
+        """y = K s on device-resident vectors: `s` and `y` are contiguous
+        float64 device tensors of shape (nvec, n) or (n,) (one slip vector per
+        row), or `(pointer, nvec)` pairs. Launches on `stream` (a
+        torch.cuda.Stream, a raw cudaStream_t, or None for the default stream)
+        and returns without synchronizing."""
+        def dev(a):
+            if isinstance(a, tuple):
+                return int(a[0]), int(a[1])
+            if a.dtype.itemsize != 8 or not a.is_contiguous() or a.shape[-1] != self.n or a.dim() > 2:
+                raise EqdArgumentError(_abi.EQD_ERR_ARG, "expected a contiguous float64 (nvec, n) device tensor")
+            return a.data_ptr(), (1 if a.dim() == 1 else a.shape[0])
+        sp, nv = dev(s)
+        yp, nvy = dev(y)
+        if nv != nvy:
+            raise EqdArgumentError(_abi.EQD_ERR_ARG, "s and y hold different numbers of vectors")
+        st = getattr(stream, "cuda_stream", stream) or 0
+        check(lib().eqd_kmat_gemv_device(self._h, C.c_void_p(sp), C.c_void_p(yp), C.c_int32(nv), C.c_void_p(st)))
+
     def close(self):
         if getattr(self, "_h", None) is not None:
             lib().eqd_kmat_destroy(self._h)

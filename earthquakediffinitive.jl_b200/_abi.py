@@ -67,7 +67,7 @@ EXPORTS = [
     "eqd_stiffness_columns", "eqd_stiffness_columns_device", "eqd_stiffness_toeplitz", "eqd_diag",
     "eqd_profile_apply", "eqd_autotune", "eqd_set_variant", "eqd_test_inject_wait_timeout", "eqd_assemble",
     "eqd_tune_chunk",
-    "eqd_kmat_create", "eqd_kmat_gemv", "eqd_kmat_destroy", "eqd_kmat_gemv_static",
+    "eqd_kmat_create", "eqd_kmat_gemv", "eqd_kmat_gemv_device", "eqd_kmat_destroy", "eqd_kmat_gemv_static",
     "eqd_server_create", "eqd_server_add_grid", "eqd_server_submit", "eqd_server_wait",
     "eqd_server_poll", "eqd_server_request_info", "eqd_server_release", "eqd_server_destroy",
     "eqd_rhs_create", "eqd_rhs_eval", "eqd_rhs_fields", "eqd_rhs_report", "eqd_rhs_destroy", "eqd_friction_solve",

@@ -406,6 +406,7 @@ struct eqd_grid {
 struct eqd_kmat {
     int device;
     int n;
+    int ks_slots = 296;  // resident CTAs of the blocked K S on the whole GPU
     DevBuf K, s, y, part;
     cudaStream_t stream = nullptr;
 };
@@ -2062,6 +2063,10 @@ extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_k
     M->n = n;
     CUDA_OR_RETURN(M->K.ensure(sizeof(double) * (size_t)n * n));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
+    int sms = 0, per_sm = 0;
+    CUDA_OR_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gemm_ks_dmma_kernel<true>, 256, 0));
+    M->ks_slots = std::max(1, sms * per_sm);
     CUDA_OR_RETURN(cudaMemcpyAsync(M->K.p, K, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
     *out = M.release();
@@ -2085,53 +2090,75 @@ static int gemv_slices(int n) {
     return std::min(s, std::max(1, n / 64));
 }
 
-// Vectors from which y = K s runs as the blocked K S (K read once per 64
-// vectors) instead of the GEMV (K read once per 4 vectors).
+// Vectors from which y = K s runs as the blocked K S on the FP64 tensor
+// cores (K read once per 64 vectors) instead of the GEMV (K read once per 4).
 static constexpr int kGemmMinVectors = 8;
 
-// Column slices of the blocked K S: enough CTAs for eight per SM (their
-// loads and the tile barriers overlap), each slice at least 256 columns of K.
-static int gemm_slices(int n, int nvec) {
-    const long long tiles = (long long)((n + kGemmBM - 1) / kGemmBM) * ((nvec + kGemmBN - 1) / kGemmBN);
-    const long long want = (8LL * 148 + tiles - 1) / tiles;
-    return (int)std::max<long long>(1, std::min<long long>(want, std::max(1, n / 256)));
+// Column slices of the blocked K S: the count (1..16, slices of at least 128
+// columns) with the least time in whole waves of resident CTAs,
+// ceil(tiles * ns / slots) / ns; the smallest count on ties.
+static int ks_slices(long long n, int nvec, int slots) {
+    const long long tiles = ((n + kDmmaBM - 1) / kDmmaBM) * ((nvec + kDmmaBN - 1) / kDmmaBN);
+    const int max_ns = (int)std::max<long long>(1, std::min<long long>(16, n / 128));
+    int best = 1;
+    double best_t = 1e300;
+    for (int ns = 1; ns <= max_ns; ++ns) {
+        const double tm = (double)((tiles * ns + slots - 1) / slots) / ns;
+        if (tm < best_t * (1.0 - 1e-9)) {
+            best_t = tm;
+            best = ns;
+        }
+    }
+    return best;
+}
+
+// y = K s for nvec device-resident vectors (s, y: n x nvec, column-major) on
+// stream st; returns after the launches. Scratch: M->part.
+static int kmat_apply(eqd_kmat *M, const double *s, double *y, int nvec, cudaStream_t st) {
+    const int n = M->n;
+    const long long ne = (long long)n * nvec;
+    const double *K = M->K.as<double>();
+    if (nvec >= kGemmMinVectors) {
+        const int ns = ks_slices(n, nvec, M->ks_slots);
+        CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)ne * ns));
+        const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + kDmmaBN - 1) / kDmmaBN));
+        if (gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n))
+            gemm_ks_dmma_kernel<true><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, M->part.as<double>());
+        else
+            gemm_ks_dmma_kernel<false><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, M->part.as<double>());
+        gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(M->part.as<double>(), n, ns, nvec, y);
+    } else {
+        const int nslice = gemv_slices(n);
+        CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)ne * nslice));
+        dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
+        launch_gemv_partial(grid, st, K, s, n, nslice, nvec, M->part.as<double>());
+        gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(M->part.as<double>(), n, nslice, nvec, y);
+    }
+    CUDA_OR_RETURN(cudaGetLastError());
+    return EQD_OK;
 }
 
 extern "C" int eqd_kmat_gemv(eqd_kmat *M, const double *s, double *y, int32_t nvec) {
     if (!M || !s || !y || nvec < 1) return fail(EQD_ERR_ARG, "invalid argument");
     CUDA_OR_RETURN(cudaSetDevice(M->device));
-    const int n = M->n;
-    if (nvec >= kGemmMinVectors) {
-        const int ns = gemm_slices(n, nvec);
-        CUDA_OR_RETURN(M->s.ensure(sizeof(double) * (size_t)n * nvec));
-        CUDA_OR_RETURN(M->y.ensure(sizeof(double) * (size_t)n * nvec));
-        CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)n * nvec * ns));
-        CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, sizeof(double) * (size_t)n * nvec, cudaMemcpyHostToDevice, M->stream));
-        const dim3 grid((unsigned)((n + kGemmBM - 1) / kGemmBM), (unsigned)ns, (unsigned)((nvec + kGemmBN - 1) / kGemmBN));
-        gemm_ks_partial_kernel<<<grid, 256, 0, M->stream>>>(M->K.as<double>(), M->s.as<double>(), n, ns, nvec,
-                                                             M->part.as<double>());
-        const long long ne = (long long)n * nvec;
-        gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, M->stream>>>(M->part.as<double>(), n, ns, nvec,
-                                                                               M->y.as<double>());
-        CUDA_OR_RETURN(cudaGetLastError());
-        CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, sizeof(double) * (size_t)n * nvec, cudaMemcpyDeviceToHost, M->stream));
-        CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
-        return EQD_OK;
-    }
-    const int nslice = gemv_slices(n);
-    CUDA_OR_RETURN(M->s.ensure(sizeof(double) * (size_t)n * nvec));
-    CUDA_OR_RETURN(M->y.ensure(sizeof(double) * (size_t)n * nvec));
-    CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)n * nvec * nslice));
-    CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, sizeof(double) * (size_t)n * nvec, cudaMemcpyHostToDevice, M->stream));
-    dim3 grid((unsigned)(((n + 1) / 2 + 255) / 256), (unsigned)nslice);
-    launch_gemv_partial(grid, M->stream, M->K.as<double>(), M->s.as<double>(), n, nslice, nvec, M->part.as<double>());
-    const long long ne = (long long)n * nvec;
-    gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, M->stream>>>(M->part.as<double>(), n, nslice, nvec,
-                                                                           M->y.as<double>());
-    CUDA_OR_RETURN(cudaGetLastError());
-    CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, sizeof(double) * (size_t)n * nvec, cudaMemcpyDeviceToHost, M->stream));
+    const size_t bytes = sizeof(double) * (size_t)M->n * nvec;
+    CUDA_OR_RETURN(M->s.ensure(bytes));
+    CUDA_OR_RETURN(M->y.ensure(bytes));
+    CUDA_OR_RETURN(cudaMemcpyAsync(M->s.p, s, bytes, cudaMemcpyHostToDevice, M->stream));
+    const int rc = kmat_apply(M, M->s.as<double>(), M->y.as<double>(), nvec, M->stream);
+    if (rc) return rc;
+    CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, bytes, cudaMemcpyDeviceToHost, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
     return EQD_OK;
+}
+
+extern "C" int eqd_kmat_gemv_device(eqd_kmat *M, const double *s_device, double *y_device, int32_t nvec,
+                                    void *stream) {
+    if (!M || !s_device || !y_device || nvec < 1) return fail(EQD_ERR_ARG, "invalid argument");
+    if ((reinterpret_cast<uintptr_t>(s_device) & 7u) || (reinterpret_cast<uintptr_t>(y_device) & 7u))
+        return fail(EQD_ERR_ARG, "s and y must be 8-byte aligned");
+    CUDA_OR_RETURN(cudaSetDevice(M->device));
+    return kmat_apply(M, s_device, y_device, nvec, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int eqd_kmat_destroy(eqd_kmat *M) {

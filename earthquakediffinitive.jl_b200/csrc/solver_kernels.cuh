@@ -847,81 +847,153 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 }
 
 // ---------------------------------------------------------------------------
-// Blocked FP64 K S for many slip vectors (Runge-Kutta stages, ensembles):
-// K is read once per 64 vectors instead of once per 4. CTA tile: 64 rows of
-// K x 64 vectors over the k-range of one column slice, in steps of 16 columns
-// staged in shared memory (each thread loads its share of the next step's
-// tiles into registers while the current step is computed); each of the 256
-// threads accumulates a 4 x 4 block
-// (rows ty + 16 i, vectors tx + 16 j) in a fixed k order. Partial sums go to
+// Blocked FP64 K S for many slip vectors (Runge-Kutta stages, ensembles) on
+// the FP64 tensor cores: K is read once per 64 vectors, and the products run
+// as mma.sync m8n8k4 f64 (D = A B + C for an 8 x 4 by 4 x 8 tile per warp
+// instruction, 512 flops), which issues 16 times fewer instructions than
+// FP64 FMAs on the CUDA cores at the same peak.
+//
+// CTA tile: 128 rows of K x 64 vectors over the k-range of one column slice,
+// in steps of 16 columns of K staged in shared memory; each thread loads its
+// share of the next step's tiles into registers while the current step is
+// computed. The eight warps form a 4 x 2 grid of 32-row x 32-vector warp
+// tiles (4 x 4 mma tiles, 32 FP64 accumulators per thread). Fragment layout
+// of m8n8k4 f64 (lane = 4 g + t): A holds A[g][t], B holds B[t][g], C and D
+// hold D[g][2t], D[g][2t + 1]. Shared-memory row strides (136 and 20
+// doubles) put the 32 lanes of a fragment read on distinct banks in two
+// wavefronts. Tails (rows past n, columns past the slice, vectors past nvec)
+// are zero-filled in registers, so every tile the tensor cores see is
+// finite. Slice bounds are multiples of 16 columns (the last ends at n), so
+// a 16-column step never crosses a slice. Partial sums go to
 // part[(v * nslice + slice) * n + row], the GEMV's layout, and the same
-// fixed-order reduction over slices finishes them.
+// fixed-order reduction over slices finishes them; the tensor cores' own
+// summation order is fixed, so results are the same bits on every run.
+// VEC2: 16-byte loads (n even, K and S 16-byte aligned).
 // ---------------------------------------------------------------------------
-constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16;
+constexpr int kDmmaBM = 128, kDmmaBN = 64, kDmmaBK = 16;
+constexpr int kDmmaAStride = kDmmaBM + 8;  // doubles per k row of the staged K tile
+constexpr int kDmmaBStride = kDmmaBK + 4;  // doubles per vector row of the staged S tile
 
-__global__ void __launch_bounds__(256) gemm_ks_partial_kernel(const double *__restrict__ K,
-                                                              const double *__restrict__ S, long long n, int nslice,
-                                                              int nvec, double *__restrict__ part) {
-    __shared__ double As[kGemmBK][kGemmBM + 1];
-    __shared__ double Bs[kGemmBK][kGemmBN + 1];
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    const long long row0 = (long long)blockIdx.x * kGemmBM;
+__host__ __device__ inline long long dmma_slice_bound(long long n, int s, int nslice) {
+    return s >= nslice ? n : (n * s / nslice) / kDmmaBK * kDmmaBK;
+}
+
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
+template <bool VEC2>
+__global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__restrict__ K,
+                                                              const double *__restrict__ S, long long n,
+                                                              int nslice, int nvec, double *__restrict__ part) {
+    __shared__ __align__(16) double As[kDmmaBK * kDmmaAStride];  // [k][row]
+    __shared__ __align__(16) double Bs[kDmmaBN * kDmmaBStride];  // [vector][k]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = warp & 3, wn = warp >> 2;
+    const long long row0 = (long long)blockIdx.x * kDmmaBM;
     const int slice = blockIdx.y;
-    const int v0 = blockIdx.z * kGemmBN;
-    const long long c0 = n * slice / nslice, c1 = n * (slice + 1) / nslice;
-    // This thread's share of a K tile (rows r, columns kk + 4 q) and of an S
-    // tile (entries kk2 of vectors j2 + 16 q), held in registers so that the
-    // next tile's loads are in flight while the current tile is used.
-    const int ar = tid % kGemmBM, akk = tid / kGemmBM;
-    const int bkk = tid % kGemmBK, bj = tid / kGemmBK;
-    double ra[4], rb[4];
+    const int v0 = blockIdx.z * kDmmaBN;
+    const long long c0 = dmma_slice_bound(n, slice, nslice), c1 = dmma_slice_bound(n, slice + 1, nslice);
+
+    // This thread's share of a step: 8 entries of the K tile, 4 of the S tile.
+    double ra[8], rb[4];
     auto load = [&](long long k0) {
+        if constexpr (VEC2) {
+            const int m = 2 * (tid & 63), kb = tid >> 6;
+            const long long row = row0 + m;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const long long row = row0 + ar, c = k0 + akk + 4 * q;
-            ra[q] = (row < n && c < c1) ? K[c * n + row] : 0.0;
-            const long long cb = k0 + bkk;
-            const int j = bj + 16 * q;
-            rb[q] = (cb < c1 && v0 + j < nvec) ? S[(long long)(v0 + j) * n + cb] : 0.0;
+            for (int q = 0; q < 4; ++q) {
+                const long long c = k0 + kb + 4 * q;
+                double2 v = make_double2(0.0, 0.0);
+                if (row < n && c < c1) v = *reinterpret_cast<const double2 *>(K + c * n + row);
+                ra[2 * q] = v.x;
+                ra[2 * q + 1] = v.y;
+            }
+            const int kk = 2 * (tid & 7), jb = tid >> 3;
+            const long long cb = k0 + kk;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int j = jb + 32 * q;
+                double2 v = make_double2(0.0, 0.0);
+                if (v0 + j < nvec && cb < c1) v = *reinterpret_cast<const double2 *>(S + (long long)(v0 + j) * n + cb);
+                rb[2 * q] = v.x;
+                rb[2 * q + 1] = v.y;
+            }
+        } else {
+            const int m = tid & 127, kb = tid >> 7;
+            const long long row = row0 + m;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const long long c = k0 + kb + 2 * q;
+                ra[q] = (row < n && c < c1) ? K[c * n + row] : 0.0;
+            }
+            const int kk = tid & 15, jb = tid >> 4;
+            const long long cb = k0 + kk;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = jb + 16 * q;
+                rb[q] = (v0 + j < nvec && cb < c1) ? S[(long long)(v0 + j) * n + cb] : 0.0;
+            }
         }
     };
-    double acc[4][4];
+    auto stage = [&]() {
+        if constexpr (VEC2) {
+            const int m = 2 * (tid & 63), kb = tid >> 6;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                *reinterpret_cast<double2 *>(&As[(kb + 4 * q) * kDmmaAStride + m]) = make_double2(ra[2 * q], ra[2 * q + 1]);
+            const int kk = 2 * (tid & 7), jb = tid >> 3;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                *reinterpret_cast<double2 *>(&Bs[(jb + 32 * q) * kDmmaBStride + kk]) = make_double2(rb[2 * q], rb[2 * q + 1]);
+        } else {
+            const int m = tid & 127, kb = tid >> 7;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) As[(kb + 2 * q) * kDmmaAStride + m] = ra[q];
+            const int kk = tid & 15, jb = tid >> 4;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Bs[(jb + 16 * q) * kDmmaBStride + kk] = rb[q];
+        }
+    };
+
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     if (c0 < c1) load(c0);
-    for (long long k0 = c0; k0 < c1; k0 += kGemmBK) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            As[akk + 4 * q][ar] = ra[q];
-            Bs[bkk][bj + 16 * q] = rb[q];
-        }
+    for (long long k0 = c0; k0 < c1; k0 += kDmmaBK) {
+        stage();
         __syncthreads();
-        if (k0 + kGemmBK < c1) load(k0 + kGemmBK);
+        if (k0 + kDmmaBK < c1) load(k0 + kDmmaBK);
 #pragma unroll
-        for (int kk = 0; kk < kGemmBK; ++kk) {
+        for (int kq = 0; kq < kDmmaBK / 4; ++kq) {
             double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+            for (int i = 0; i < 4; ++i) a[i] = As[(kq * 4 + t) * kDmmaAStride + wm * 32 + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + g) * kDmmaBStride + kq * 4 + t];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const long long row = row0 + ty + 16 * i;
+        const long long row = row0 + wm * 32 + i * 8 + g;
         if (row >= n) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int v = v0 + tx + 16 * j;
-            if (v < nvec) part[((long long)v * nslice + slice) * n + row] = acc[i][j];
-        }
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int v = v0 + wn * 32 + j * 8 + 2 * t + e;
+                if (v < nvec) part[((long long)v * nslice + slice) * n + row] = acc[i][j][e];
+            }
     }
 }
 

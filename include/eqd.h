@@ -231,10 +231,21 @@ int eqd_assemble(eqd_grid *grid, int32_t which, int64_t capacity, int64_t *indpt
 int eqd_diag(eqd_grid *grid, double *d);
 
 /* Time-loop GEMV `mul!(Δτ, K, slip)` (src/BP8.jl:366) ----------------------
- * K stays resident on the device; y = K s for nvec vectors (n x nvec each),
- * any n >= 1. */
+ * K stays resident on the device; y = K s for nvec vectors (n x nvec each,
+ * column-major), any n >= 1. From 8 vectors on, K S runs blocked on the FP64
+ * tensor cores (K read once per 64 vectors); fewer run as the GEMV. s and y
+ * are host arrays; the call copies them and returns when y is written. */
 int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out);
 int eqd_kmat_gemv(eqd_kmat *kmat, const double *s, double *y, int32_t nvec);
+/* The same y = K s with s and y DEVICE pointers (8-byte aligned, on the
+ * kmat's device) for callers whose slip vectors are already resident, e.g.
+ * Runge-Kutta stages of a time loop on the GPU (no counterpart in the
+ * reference, which multiplies host arrays). Launches on `stream` (a
+ * cudaStream_t, NULL = default stream) and returns without synchronizing.
+ * Partial sums live in scratch owned by the kmat: calls on one kmat must be
+ * serialised (one stream, or events), and the first call with a given n * nvec
+ * may allocate it (make that call before any stream capture). */
+int eqd_kmat_gemv_device(eqd_kmat *kmat, const double *s_device, double *y_device, int32_t nvec, void *stream);
 int eqd_kmat_destroy(eqd_kmat *kmat);
 
 /* Allocation-free y = K s (no counterpart in the reference: an addition for
