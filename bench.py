@@ -454,7 +454,7 @@ def main():
     if ncols == 2 * nf:
         n = 2 * nf
         nv = 64
-        Sm = np.random.default_rng(2).standard_normal((n, nv))
+        Sm = np.asfortranarray(np.random.default_rng(2).standard_normal((n, nv)))  # column-major, as a Julia caller holds it
         KM = eqd.KMatrix(Kmix)
         KM.gemv(Sm)
         reps = 5

@@ -454,14 +454,18 @@ class KMatrix:
         self._h = h
 
     def gemv(self, s):
-        s = f64(s)
+        """y = K s for one slip vector (n,) or several (n, nvec). A
+        column-major (Fortran-ordered) (n, nvec) array goes to the device
+        without a host transpose; the result of a matrix product is returned
+        column-major."""
+        s = np.asarray(s, dtype=np.float64)
         one = s.ndim == 1
         S = np.ascontiguousarray((s.reshape(-1, 1) if one else s).T)
         if S.shape[1] != self.n:
             raise EqdArgumentError(_abi.EQD_ERR_ARG, "slip length does not match K")
         Y = np.empty_like(S)
         check(lib().eqd_kmat_gemv(self._h, ptr(S), ptr(Y), C.c_int32(S.shape[0])))
-        return Y[0].copy() if one else Y.T.copy()
+        return Y[0] if one else Y.T
 
     def gemv_device(self, s, y, stream=None):
         """y = K s on device-resident vectors: `s` and `y` are contiguous

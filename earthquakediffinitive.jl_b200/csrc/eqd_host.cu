@@ -406,7 +406,7 @@ struct eqd_grid {
 struct eqd_kmat {
     int device;
     int n;
-    int ks_slots = 296;  // resident CTAs of the blocked K S on the whole GPU
+    int ks_slots[3] = {296, 296, 296};  // resident CTAs of the blocked K S (16, 32, 64 vectors per CTA)
     DevBuf K, s, y, part;
     cudaStream_t stream = nullptr;
 };
@@ -2063,10 +2063,12 @@ extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_k
     M->n = n;
     CUDA_OR_RETURN(M->K.ensure(sizeof(double) * (size_t)n * n));
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
-    int sms = 0, per_sm = 0;
+    int sms = 0, per_sm[3] = {0, 0, 0};
     CUDA_OR_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gemm_ks_dmma_kernel<true>, 256, 0));
-    M->ks_slots = std::max(1, sms * per_sm);
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], gemm_ks_dmma_kernel<true, 1>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], gemm_ks_dmma_kernel<true, 2>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], gemm_ks_dmma_kernel<true, 4>, 256, 0));
+    for (int k = 0; k < 3; ++k) M->ks_slots[k] = std::max(1, sms * per_sm[k]);
     CUDA_OR_RETURN(cudaMemcpyAsync(M->K.p, K, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
     *out = M.release();
@@ -2097,8 +2099,8 @@ static constexpr int kGemmMinVectors = 8;
 // Column slices of the blocked K S: the count (1..16, slices of at least 128
 // columns) with the least time in whole waves of resident CTAs,
 // ceil(tiles * ns / slots) / ns; the smallest count on ties.
-static int ks_slices(long long n, int nvec, int slots) {
-    const long long tiles = ((n + kDmmaBM - 1) / kDmmaBM) * ((nvec + kDmmaBN - 1) / kDmmaBN);
+static int ks_slices(long long n, int nvec, int bn, int slots) {
+    const long long tiles = ((n + kDmmaBM - 1) / kDmmaBM) * ((nvec + bn - 1) / bn);
     const int max_ns = (int)std::max<long long>(1, std::min<long long>(16, n / 128));
     int best = 1;
     double best_t = 1e300;
@@ -2119,13 +2121,18 @@ static int kmat_apply(eqd_kmat *M, const double *s, double *y, int nvec, cudaStr
     const long long ne = (long long)n * nvec;
     const double *K = M->K.as<double>();
     if (nvec >= kGemmMinVectors) {
-        const int ns = ks_slices(n, nvec, M->ks_slots);
+        // Vector tile: 16, 32 or 64 vectors per CTA, the narrowest that holds nvec.
+        const int tk = nvec <= 16 ? 0 : nvec <= 32 ? 1 : 2, bn = 16 << tk;
+        const int ns = ks_slices(n, nvec, bn, M->ks_slots[tk]);
         CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)ne * ns));
-        const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + kDmmaBN - 1) / kDmmaBN));
-        if (gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n))
-            gemm_ks_dmma_kernel<true><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, M->part.as<double>());
-        else
-            gemm_ks_dmma_kernel<false><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, M->part.as<double>());
+        const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + bn - 1) / bn));
+        const bool v2 = gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n);
+        double *pp = M->part.as<double>();
+#define EQD_KS(V, NT) gemm_ks_dmma_kernel<V, NT><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, pp)
+        if (tk == 0) { if (v2) EQD_KS(true, 1); else EQD_KS(false, 1); }
+        else if (tk == 1) { if (v2) EQD_KS(true, 2); else EQD_KS(false, 2); }
+        else { if (v2) EQD_KS(true, 4); else EQD_KS(false, 4); }
+#undef EQD_KS
         gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(M->part.as<double>(), n, ns, nvec, y);
     } else {
         const int nslice = gemv_slices(n);

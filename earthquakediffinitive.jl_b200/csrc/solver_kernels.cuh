@@ -853,11 +853,12 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // instruction, 512 flops), which issues 16 times fewer instructions than
 // FP64 FMAs on the CUDA cores at the same peak.
 //
-// CTA tile: 128 rows of K x 64 vectors over the k-range of one column slice,
-// in steps of 16 columns of K staged in shared memory; each thread loads its
-// share of the next step's tiles into registers while the current step is
-// computed. The eight warps form a 4 x 2 grid of 32-row x 32-vector warp
-// tiles (4 x 4 mma tiles, 32 FP64 accumulators per thread). Fragment layout
+// CTA tile: 128 rows of K x 16 NT vectors (NT = 1, 2, 4: 16, 32 or 64) over
+// the k-range of one column slice, in steps of 16 columns of K staged in
+// shared memory; each thread loads its share of the next step's tiles into
+// registers while the current step is computed. The eight warps form a 4 x 2
+// grid of 32-row x 8 NT-vector warp tiles (4 x NT mma tiles, 8 NT FP64
+// accumulators per thread). Fragment layout
 // of m8n8k4 f64 (lane = 4 g + t): A holds A[g][t], B holds B[t][g], C and D
 // hold D[g][2t], D[g][2t + 1]. Shared-memory row strides (136 and 20
 // doubles) put the 32 lanes of a fragment read on distinct banks in two
@@ -870,7 +871,7 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // summation order is fixed, so results are the same bits on every run.
 // VEC2: 16-byte loads (n even, K and S 16-byte aligned).
 // ---------------------------------------------------------------------------
-constexpr int kDmmaBM = 128, kDmmaBN = 64, kDmmaBK = 16;
+constexpr int kDmmaBM = 128, kDmmaBK = 16;
 constexpr int kDmmaAStride = kDmmaBM + 8;  // doubles per k row of the staged K tile
 constexpr int kDmmaBStride = kDmmaBK + 4;  // doubles per vector row of the staged S tile
 
@@ -884,21 +885,24 @@ __device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) 
         : "d"(a), "d"(b));
 }
 
-template <bool VEC2>
+template <bool VEC2, int NT>
 __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__restrict__ K,
                                                               const double *__restrict__ S, long long n,
                                                               int nslice, int nvec, double *__restrict__ part) {
+    constexpr int BN = 16 * NT;                                  // vectors per CTA
+    constexpr int BPAIRS = BN * kDmmaBK / 2;                     // 16-byte pairs of an S tile
+    constexpr int BQ2 = (BPAIRS + 255) / 256, BQ1 = BN * kDmmaBK / 256;
     __shared__ __align__(16) double As[kDmmaBK * kDmmaAStride];  // [k][row]
-    __shared__ __align__(16) double Bs[kDmmaBN * kDmmaBStride];  // [vector][k]
+    __shared__ __align__(16) double Bs[BN * kDmmaBStride];       // [vector][k]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp & 3, wn = warp >> 2;
     const long long row0 = (long long)blockIdx.x * kDmmaBM;
     const int slice = blockIdx.y;
-    const int v0 = blockIdx.z * kDmmaBN;
+    const int v0 = blockIdx.z * BN;
     const long long c0 = dmma_slice_bound(n, slice, nslice), c1 = dmma_slice_bound(n, slice + 1, nslice);
 
-    // This thread's share of a step: 8 entries of the K tile, 4 of the S tile.
+    // This thread's share of a step: 8 entries of the K tile, up to 4 of the S tile.
     double ra[8], rb[4];
     auto load = [&](long long k0) {
         if constexpr (VEC2) {
@@ -912,13 +916,13 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
                 ra[2 * q] = v.x;
                 ra[2 * q + 1] = v.y;
             }
-            const int kk = 2 * (tid & 7), jb = tid >> 3;
-            const long long cb = k0 + kk;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int j = jb + 32 * q;
+            for (int q = 0; q < BQ2; ++q) {
+                const int pidx = tid + 256 * q, j = pidx >> 3;
+                const long long cb = k0 + 2 * (pidx & 7);
                 double2 v = make_double2(0.0, 0.0);
-                if (v0 + j < nvec && cb < c1) v = *reinterpret_cast<const double2 *>(S + (long long)(v0 + j) * n + cb);
+                if (pidx < BPAIRS && v0 + j < nvec && cb < c1)
+                    v = *reinterpret_cast<const double2 *>(S + (long long)(v0 + j) * n + cb);
                 rb[2 * q] = v.x;
                 rb[2 * q + 1] = v.y;
             }
@@ -930,11 +934,10 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
                 const long long c = k0 + kb + 2 * q;
                 ra[q] = (row < n && c < c1) ? K[c * n + row] : 0.0;
             }
-            const int kk = tid & 15, jb = tid >> 4;
-            const long long cb = k0 + kk;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = jb + 16 * q;
+            for (int q = 0; q < BQ1; ++q) {
+                const int e = tid + 256 * q, j = e >> 4;
+                const long long cb = k0 + (e & 15);
                 rb[q] = (v0 + j < nvec && cb < c1) ? S[(long long)(v0 + j) * n + cb] : 0.0;
             }
         }
@@ -945,25 +948,30 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 *reinterpret_cast<double2 *>(&As[(kb + 4 * q) * kDmmaAStride + m]) = make_double2(ra[2 * q], ra[2 * q + 1]);
-            const int kk = 2 * (tid & 7), jb = tid >> 3;
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
-                *reinterpret_cast<double2 *>(&Bs[(jb + 32 * q) * kDmmaBStride + kk]) = make_double2(rb[2 * q], rb[2 * q + 1]);
+            for (int q = 0; q < BQ2; ++q) {
+                const int pidx = tid + 256 * q;
+                if (pidx < BPAIRS)
+                    *reinterpret_cast<double2 *>(&Bs[(pidx >> 3) * kDmmaBStride + 2 * (pidx & 7)]) =
+                        make_double2(rb[2 * q], rb[2 * q + 1]);
+            }
         } else {
             const int m = tid & 127, kb = tid >> 7;
 #pragma unroll
             for (int q = 0; q < 8; ++q) As[(kb + 2 * q) * kDmmaAStride + m] = ra[q];
-            const int kk = tid & 15, jb = tid >> 4;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) Bs[(jb + 16 * q) * kDmmaBStride + kk] = rb[q];
+            for (int q = 0; q < BQ1; ++q) {
+                const int e = tid + 256 * q;
+                Bs[(e >> 4) * kDmmaBStride + (e & 15)] = rb[q];
+            }
         }
     };
 
-    double acc[4][4][2];
+    double acc[4][NT][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     if (c0 < c1) load(c0);
     for (long long k0 = c0; k0 < c1; k0 += kDmmaBK) {
         stage();
@@ -971,15 +979,15 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
         if (k0 + kDmmaBK < c1) load(k0 + kDmmaBK);
 #pragma unroll
         for (int kq = 0; kq < kDmmaBK / 4; ++kq) {
-            double a[4], b[4];
+            double a[4], b[NT];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = As[(kq * 4 + t) * kDmmaAStride + wm * 32 + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + g) * kDmmaBStride + kq * 4 + t];
+            for (int j = 0; j < NT; ++j) b[j] = Bs[(wn * 8 * NT + j * 8 + g) * kDmmaBStride + kq * 4 + t];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
+                for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
         }
         __syncthreads();
     }
@@ -988,10 +996,10 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
         const long long row = row0 + wm * 32 + i * 8 + g;
         if (row >= n) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NT; ++j)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-                const int v = v0 + wn * 32 + j * 8 + 2 * t + e;
+                const int v = v0 + wn * 8 * NT + j * 8 + 2 * t + e;
                 if (v < nvec) part[((long long)v * nslice + slice) * n + row] = acc[i][j][e];
             }
     }

@@ -163,15 +163,18 @@ def test_bp8_dz100_model(eqd):
     assert rel(K, K_ref) < K_TOL
 
 
-@pytest.mark.parametrize("n, nvec", [(578, 8), (1155, 64), (2178, 70)])
+@pytest.mark.parametrize("n, nvec", [(578, 8), (1155, 64), (2178, 70), (1155, 12), (1155, 20), (4356, 24), (4356, 130)])
 def test_batched_ks(eqd, n, nvec):
-    """y = K S for many slip vectors (the blocked K S path, K read once per
-    64 vectors) against numpy FP64, relative to |K||S|."""
+    """y = K S for many slip vectors (the blocked K S on the FP64 tensor
+    cores: 16-, 32- and 64-vector tiles, odd n on 8-byte loads, more than 64
+    vectors over several tiles) against numpy FP64, relative to |K||S|; the
+    Fortran-ordered input gives the same bits as the C-ordered one."""
     rng = np.random.default_rng(n)
     K = rng.standard_normal((n, n))
     S = rng.standard_normal((n, nvec))
     M = eqd.KMatrix(K)
     Y = M.gemv(S)
+    assert np.array_equal(M.gemv(np.asfortranarray(S)), Y)
     M.close()
     scale = abs(K).dot(abs(S)).max()
     assert Y.shape == (n, nvec)
