@@ -2065,9 +2065,9 @@ extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_k
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
     int sms = 0, per_sm[3] = {0, 0, 0};
     CUDA_OR_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], gemm_ks_dmma_kernel<true, 1>, 256, 0));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], gemm_ks_dmma_kernel<true, 2>, 256, 0));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], gemm_ks_dmma_kernel<true, 4>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], gemm_ks_dmma_kernel<true, 1, 32>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], gemm_ks_dmma_kernel<true, 2, 32>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], gemm_ks_dmma_kernel<true, 4, 16>, 256, 0));
     for (int k = 0; k < 3; ++k) M->ks_slots[k] = std::max(1, sms * per_sm[k]);
     CUDA_OR_RETURN(cudaMemcpyAsync(M->K.p, K, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
@@ -2093,8 +2093,10 @@ static int gemv_slices(int n) {
 }
 
 // Vectors from which y = K s runs as the blocked K S on the FP64 tensor
-// cores (K read once per 64 vectors) instead of the GEMV (K read once per 4).
-static constexpr int kGemmMinVectors = 8;
+// cores (K read once per 16-64 vectors) instead of the GEMV (K read once per
+// 4). Measured at n = 13,122: GEMV 0.25 / 0.25 / 0.32 / 0.44 ms for 1-4
+// vectors (1.1-1.8 ms for 5-8), the tensor-core path 0.31-0.32 ms for 2-8.
+static constexpr int kGemmMinVectors = 3;
 
 // Column slices of the blocked K S: the count (1..16, slices of at least 128
 // columns) with the least time in whole waves of resident CTAs,
@@ -2128,7 +2130,7 @@ static int kmat_apply(eqd_kmat *M, const double *s, double *y, int nvec, cudaStr
         const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + bn - 1) / bn));
         const bool v2 = gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n);
         double *pp = M->part.as<double>();
-#define EQD_KS(V, NT) gemm_ks_dmma_kernel<V, NT><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, pp)
+#define EQD_KS(V, NT) gemm_ks_dmma_kernel<V, NT, (NT < 4 ? 32 : 16)><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, pp)
         if (tk == 0) { if (v2) EQD_KS(true, 1); else EQD_KS(false, 1); }
         else if (tk == 1) { if (v2) EQD_KS(true, 2); else EQD_KS(false, 2); }
         else { if (v2) EQD_KS(true, 4); else EQD_KS(false, 4); }

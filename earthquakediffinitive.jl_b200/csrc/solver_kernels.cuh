@@ -854,18 +854,19 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // FP64 FMAs on the CUDA cores at the same peak.
 //
 // CTA tile: 128 rows of K x 16 NT vectors (NT = 1, 2, 4: 16, 32 or 64) over
-// the k-range of one column slice, in steps of 16 columns of K staged in
+// the k-range of one column slice, in steps of KB columns of K (16, or 32 for
+// the narrow tiles, whose K stream needs more bytes in flight) staged in
 // shared memory; each thread loads its share of the next step's tiles into
 // registers while the current step is computed. The eight warps form a 4 x 2
 // grid of 32-row x 8 NT-vector warp tiles (4 x NT mma tiles, 8 NT FP64
 // accumulators per thread). Fragment layout
 // of m8n8k4 f64 (lane = 4 g + t): A holds A[g][t], B holds B[t][g], C and D
-// hold D[g][2t], D[g][2t + 1]. Shared-memory row strides (136 and 20
+// hold D[g][2t], D[g][2t + 1]. Shared-memory row strides (136 and KB + 4
 // doubles) put the 32 lanes of a fragment read on distinct banks in two
 // wavefronts. Tails (rows past n, columns past the slice, vectors past nvec)
 // are zero-filled in registers, so every tile the tensor cores see is
-// finite. Slice bounds are multiples of 16 columns (the last ends at n), so
-// a 16-column step never crosses a slice. Partial sums go to
+// finite; that includes the columns of a step that lie past the slice's end.
+// Slice bounds are multiples of 16 columns (the last ends at n). Partial sums go to
 // part[(v * nslice + slice) * n + row], the GEMV's layout, and the same
 // fixed-order reduction over slices finishes them; the tensor cores' own
 // summation order is fixed, so results are the same bits on every run.
@@ -873,7 +874,6 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // ---------------------------------------------------------------------------
 constexpr int kDmmaBM = 128, kDmmaBK = 16;
 constexpr int kDmmaAStride = kDmmaBM + 8;  // doubles per k row of the staged K tile
-constexpr int kDmmaBStride = kDmmaBK + 4;  // doubles per vector row of the staged S tile
 
 __host__ __device__ inline long long dmma_slice_bound(long long n, int s, int nslice) {
     return s >= nslice ? n : (n * s / nslice) / kDmmaBK * kDmmaBK;
@@ -885,15 +885,16 @@ __device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) 
         : "d"(a), "d"(b));
 }
 
-template <bool VEC2, int NT>
+template <bool VEC2, int NT, int KB>
 __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__restrict__ K,
                                                               const double *__restrict__ S, long long n,
                                                               int nslice, int nvec, double *__restrict__ part) {
     constexpr int BN = 16 * NT;                                  // vectors per CTA
-    constexpr int BPAIRS = BN * kDmmaBK / 2;                     // 16-byte pairs of an S tile
-    constexpr int BQ2 = (BPAIRS + 255) / 256, BQ1 = BN * kDmmaBK / 256;
-    __shared__ __align__(16) double As[kDmmaBK * kDmmaAStride];  // [k][row]
-    __shared__ __align__(16) double Bs[BN * kDmmaBStride];       // [vector][k]
+    constexpr int BST = KB + 4;                                  // doubles per vector row of the S tile
+    constexpr int BPAIRS = BN * KB / 2;                          // 16-byte pairs of an S tile
+    constexpr int BQ2 = (BPAIRS + 255) / 256, BQ1 = BN * KB / 256;
+    __shared__ __align__(16) double As[KB * kDmmaAStride];       // [k][row]
+    __shared__ __align__(16) double Bs[BN * BST];                // [vector][k]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp & 3, wn = warp >> 2;
@@ -902,14 +903,14 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
     const int v0 = blockIdx.z * BN;
     const long long c0 = dmma_slice_bound(n, slice, nslice), c1 = dmma_slice_bound(n, slice + 1, nslice);
 
-    // This thread's share of a step: 8 entries of the K tile, up to 4 of the S tile.
-    double ra[8], rb[4];
+    // This thread's share of a step: KB / 2 entries of the K tile, up to 4 of the S tile.
+    double ra[KB / 2], rb[4];
     auto load = [&](long long k0) {
         if constexpr (VEC2) {
             const int m = 2 * (tid & 63), kb = tid >> 6;
             const long long row = row0 + m;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < KB / 4; ++q) {
                 const long long c = k0 + kb + 4 * q;
                 double2 v = make_double2(0.0, 0.0);
                 if (row < n && c < c1) v = *reinterpret_cast<const double2 *>(K + c * n + row);
@@ -918,8 +919,8 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
             }
 #pragma unroll
             for (int q = 0; q < BQ2; ++q) {
-                const int pidx = tid + 256 * q, j = pidx >> 3;
-                const long long cb = k0 + 2 * (pidx & 7);
+                const int pidx = tid + 256 * q, j = pidx / (KB / 2);
+                const long long cb = k0 + 2 * (pidx % (KB / 2));
                 double2 v = make_double2(0.0, 0.0);
                 if (pidx < BPAIRS && v0 + j < nvec && cb < c1)
                     v = *reinterpret_cast<const double2 *>(S + (long long)(v0 + j) * n + cb);
@@ -930,14 +931,14 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
             const int m = tid & 127, kb = tid >> 7;
             const long long row = row0 + m;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
+            for (int q = 0; q < KB / 2; ++q) {
                 const long long c = k0 + kb + 2 * q;
                 ra[q] = (row < n && c < c1) ? K[c * n + row] : 0.0;
             }
 #pragma unroll
             for (int q = 0; q < BQ1; ++q) {
-                const int e = tid + 256 * q, j = e >> 4;
-                const long long cb = k0 + (e & 15);
+                const int e = tid + 256 * q, j = e / KB;
+                const long long cb = k0 + (e % KB);
                 rb[q] = (v0 + j < nvec && cb < c1) ? S[(long long)(v0 + j) * n + cb] : 0.0;
             }
         }
@@ -946,44 +947,43 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
         if constexpr (VEC2) {
             const int m = 2 * (tid & 63), kb = tid >> 6;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < KB / 4; ++q)
                 *reinterpret_cast<double2 *>(&As[(kb + 4 * q) * kDmmaAStride + m]) = make_double2(ra[2 * q], ra[2 * q + 1]);
 #pragma unroll
             for (int q = 0; q < BQ2; ++q) {
                 const int pidx = tid + 256 * q;
                 if (pidx < BPAIRS)
-                    *reinterpret_cast<double2 *>(&Bs[(pidx >> 3) * kDmmaBStride + 2 * (pidx & 7)]) =
+                    *reinterpret_cast<double2 *>(&Bs[(pidx / (KB / 2)) * BST + 2 * (pidx % (KB / 2))]) =
                         make_double2(rb[2 * q], rb[2 * q + 1]);
             }
         } else {
             const int m = tid & 127, kb = tid >> 7;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) As[(kb + 2 * q) * kDmmaAStride + m] = ra[q];
+            for (int q = 0; q < KB / 2; ++q) As[(kb + 2 * q) * kDmmaAStride + m] = ra[q];
 #pragma unroll
             for (int q = 0; q < BQ1; ++q) {
                 const int e = tid + 256 * q;
-                Bs[(e >> 4) * kDmmaBStride + (e & 15)] = rb[q];
+                Bs[(e / KB) * BST + (e % KB)] = rb[q];
             }
         }
     };
-
     double acc[4][NT][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     if (c0 < c1) load(c0);
-    for (long long k0 = c0; k0 < c1; k0 += kDmmaBK) {
+    for (long long k0 = c0; k0 < c1; k0 += KB) {
         stage();
         __syncthreads();
-        if (k0 + kDmmaBK < c1) load(k0 + kDmmaBK);
+        if (k0 + KB < c1) load(k0 + KB);
 #pragma unroll
-        for (int kq = 0; kq < kDmmaBK / 4; ++kq) {
+        for (int kq = 0; kq < KB / 4; ++kq) {
             double a[4], b[NT];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = As[(kq * 4 + t) * kDmmaAStride + wm * 32 + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < NT; ++j) b[j] = Bs[(wn * 8 * NT + j * 8 + g) * kDmmaBStride + kq * 4 + t];
+            for (int j = 0; j < NT; ++j) b[j] = Bs[(wn * 8 * NT + j * 8 + g) * BST + kq * 4 + t];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll

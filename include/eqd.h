@@ -232,7 +232,7 @@ int eqd_diag(eqd_grid *grid, double *d);
 
 /* Time-loop GEMV `mul!(Δτ, K, slip)` (src/BP8.jl:366) ----------------------
  * K stays resident on the device; y = K s for nvec vectors (n x nvec each,
- * column-major), any n >= 1. From 8 vectors on, K S runs blocked on the FP64
+ * column-major), any n >= 1. From 3 vectors on, K S runs blocked on the FP64
  * tensor cores (K read once per 64 vectors); fewer run as the GEMV. s and y
  * are host arrays; the call copies them and returns when y is written. */
 int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_kmat **out);

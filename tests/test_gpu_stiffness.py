@@ -216,7 +216,7 @@ def test_gemv(eqd):
     s = rng.standard_normal(n)
     y = M.gemv(s)
     assert np.allclose(y, K @ s, rtol=1e-12, atol=1e-12 * abs(K).sum(1).max())
-    for nv in (3, 4, 9):  # vector groups of four, with remainders
+    for nv in (2, 3, 4, 9):  # the GEMV (1-2 vectors) and the tensor-core K S (3+)
         S = rng.standard_normal((n, nv))
         Y = M.gemv(S)
         assert np.allclose(Y, K @ S, rtol=1e-12, atol=1e-10)
