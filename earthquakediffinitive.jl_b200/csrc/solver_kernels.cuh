@@ -859,21 +859,23 @@ __global__ void __launch_bounds__(256) gemv_partial_kernel(const double *__restr
 // shared memory; each thread loads its share of the next step's tiles into
 // registers while the current step is computed. The eight warps form a 4 x 2
 // grid of 32-row x 8 NT-vector warp tiles (4 x NT mma tiles, 8 NT FP64
-// accumulators per thread). Fragment layout
-// of m8n8k4 f64 (lane = 4 g + t): A holds A[g][t], B holds B[t][g], C and D
-// hold D[g][2t], D[g][2t + 1]. Shared-memory row strides (136 and KB + 4
-// doubles) put the 32 lanes of a fragment read on distinct banks in two
-// wavefronts. Tails (rows past n, columns past the slice, vectors past nvec)
-// are zero-filled in registers, so every tile the tensor cores see is
-// finite; that includes the columns of a step that lie past the slice's end.
-// Slice bounds are multiples of 16 columns (the last ends at n). Partial sums go to
-// part[(v * nslice + slice) * n + row], the GEMV's layout, and the same
-// fixed-order reduction over slices finishes them; the tensor cores' own
-// summation order is fixed, so results are the same bits on every run.
+// accumulators per thread). Fragment layout of m8n8k4 f64 (lane = 4 g + t):
+// A holds A[g][t], B holds B[t][g], C and D hold D[g][2t], D[g][2t + 1]. A
+// 64-bit shared load is served per half-warp (g = 0..3 or 4..7, t = 0..3):
+// row strides of 132 and KB + 4 doubles put the 16 doubles of each half on
+// distinct banks (A: offsets 4t + g mod 16; B: 20 g + t or 36 g + t), so a
+// fragment read takes two wavefronts. Tails (rows past n, columns past the
+// slice, vectors past nvec) are zero-filled in registers, so every tile the
+// tensor cores see is finite; that includes the columns of a step that lie
+// past the slice's end. Slice bounds are multiples of 16 columns (the last
+// ends at n). Partial sums go to part[(v * nslice + slice) * n + row], the
+// GEMV's layout, and the same fixed-order reduction over slices finishes
+// them; the tensor cores' own summation order is fixed, so results are the
+// same bits on every run.
 // VEC2: 16-byte loads (n even, K and S 16-byte aligned).
 // ---------------------------------------------------------------------------
 constexpr int kDmmaBM = 128, kDmmaBK = 16;
-constexpr int kDmmaAStride = kDmmaBM + 8;  // doubles per k row of the staged K tile
+constexpr int kDmmaAStride = kDmmaBM + 4;  // doubles per k row of the staged K tile
 
 __host__ __device__ inline long long dmma_slice_bound(long long n, int s, int nslice) {
     return s >= nslice ? n : (n * s / nslice) / kDmmaBK * kDmmaBK;
