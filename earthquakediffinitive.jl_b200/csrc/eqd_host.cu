@@ -2095,7 +2095,7 @@ static int gemv_slices(int n) {
 // Vectors from which y = K s runs as the blocked K S on the FP64 tensor
 // cores (K read once per 16-64 vectors) instead of the GEMV (K read once per
 // 4). Measured at n = 13,122: GEMV 0.25 / 0.25 / 0.32 / 0.44 ms for 1-4
-// vectors (1.1-1.8 ms for 5-8), the tensor-core path 0.31-0.32 ms for 2-8.
+// vectors (1.1-1.8 ms for 5-8), the tensor-core path 0.27-0.32 ms for 2-8.
 static constexpr int kGemmMinVectors = 3;
 
 // Column slices of the blocked K S: the count (1..16, slices of at least 128
