@@ -13,7 +13,7 @@ module EqdB200
 using LinearAlgebra
 
 export GpuFaultElasticity, gpu_fault_stiffness, gpu_fault_stiffness_toeplitz,
-       gpu_shear_traction, GpuK, gpu_mul!, gpu_solver_report,
+       gpu_shear_traction, GpuK, gpu_mul!, gpu_mul_device!, gpu_solver_report,
        GpuServer, serve!, submit, wait_request, request_info, GpuSplitNodeOperator
 
 const libeqd = get(ENV, "EQD_LIB", joinpath(@__DIR__, "..", "lib", "libeqd.so"))
@@ -199,6 +199,29 @@ function gpu_mul!(y::Vector{Float64}, K::GpuK, s::Vector{Float64})
     check(ccall((:eqd_kmat_gemv, libeqd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
                 K.handle, s, y, 1))
     return y
+end
+
+"`Y = K S` for the columns of `S` (n x nvec; from 3 columns on, on the FP64 tensor cores)."
+function gpu_mul!(Y::Matrix{Float64}, K::GpuK, S::Matrix{Float64})
+    size(S, 1) == K.n && size(Y) == size(S) || throw(DimensionMismatch("K is $(K.n) x $(K.n), S $(size(S)), Y $(size(Y))"))
+    check(ccall((:eqd_kmat_gemv, libeqd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
+                K.handle, S, Y, size(S, 2)))
+    return Y
+end
+
+"""
+    gpu_mul_device!(y_ptr, K, s_ptr, nvec; stream=C_NULL)
+
+`y = K s` on slip vectors already on the device (e.g. `pointer(s)` of a
+`CuMatrix{Float64}` of n x nvec, column-major), launched on `stream` (a
+`CUstream` handle) without a synchronize. Calls on one `GpuK` must be
+serialised; the first call of a size may allocate scratch (make it before
+stream capture).
+"""
+function gpu_mul_device!(y_ptr, K::GpuK, s_ptr, nvec::Integer; stream=C_NULL)
+    check(ccall((:eqd_kmat_gemv_device, libeqd), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int32, Ptr{Cvoid}),
+                K.handle, Ptr{Cvoid}(UInt(s_ptr)), Ptr{Cvoid}(UInt(y_ptr)), nvec, Ptr{Cvoid}(UInt(stream))))
+    return y_ptr
 end
 
 # ---------------------------------------------------------------------------
