@@ -406,9 +406,8 @@ struct eqd_grid {
 struct eqd_kmat {
     int device;
     int n;
-    int ks_slots = 296;                 // resident CTAs of the blocked K S, 64 vectors per CTA
-    int ring_slots[2] = {148, 148};     // and of its bulk-copy ring form (16, 32 vectors per CTA)
-    DevBuf K, s, y, part, err;
+    int ks_slots[3] = {296, 296, 296};  // resident CTAs of the blocked K S (16, 32, 64 vectors per CTA)
+    DevBuf K, s, y, part;
     cudaStream_t stream = nullptr;
 };
 
@@ -2066,22 +2065,10 @@ extern "C" int eqd_kmat_create(int32_t device, int32_t n, const double *K, eqd_k
     CUDA_OR_RETURN(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
     int sms = 0, per_sm[3] = {0, 0, 0};
     CUDA_OR_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], gemm_ks_dmma_kernel<true, 1, 32>, 256, 0));
+    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], gemm_ks_dmma_kernel<true, 2, 32>, 256, 0));
     CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], gemm_ks_dmma_kernel<true, 4, 16>, 256, 0));
-    M->ks_slots = std::max(1, sms * per_sm[2]);
-    using R1 = KsRing<1, 32, 4>;
-    using R2 = KsRing<2, 32, 4>;
-    CUDA_OR_RETURN(cudaFuncSetAttribute(gemm_ks_dmma_ring_kernel<1, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)R1::SMEM));
-    CUDA_OR_RETURN(cudaFuncSetAttribute(gemm_ks_dmma_ring_kernel<2, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)R2::SMEM));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], gemm_ks_dmma_ring_kernel<1, 32, 4>, 256,
-                                                                 R1::SMEM));
-    CUDA_OR_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], gemm_ks_dmma_ring_kernel<2, 32, 4>, 256,
-                                                                 R2::SMEM));
-    M->ring_slots[0] = std::max(1, sms * per_sm[0]);
-    M->ring_slots[1] = std::max(1, sms * per_sm[1]);
-    CUDA_OR_RETURN(M->err.ensure(sizeof(unsigned)));
-    CUDA_OR_RETURN(cudaMemset(M->err.p, 0, sizeof(unsigned)));
+    for (int k = 0; k < 3; ++k) M->ks_slots[k] = std::max(1, sms * per_sm[k]);
     CUDA_OR_RETURN(cudaMemcpyAsync(M->K.p, K, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
     *out = M.release();
@@ -2136,32 +2123,18 @@ static int kmat_apply(eqd_kmat *M, const double *s, double *y, int nvec, cudaStr
     const long long ne = (long long)n * nvec;
     const double *K = M->K.as<double>();
     if (nvec >= kGemmMinVectors) {
-        // Vector tile: 16, 32 or 64 vectors per CTA, the narrowest that holds
-        // nvec. The narrow tiles stream K through the bulk-copy ring where
-        // 16-byte copies are possible.
+        // Vector tile: 16, 32 or 64 vectors per CTA, the narrowest that holds nvec.
         const int tk = nvec <= 16 ? 0 : nvec <= 32 ? 1 : 2, bn = 16 << tk;
-        const bool v2 = gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n);
-        const bool ring = v2 && tk < 2;
-        // The slice count depends only on n, nvec and the tile (the ring's
-        // occupancy for the narrow tiles on either load path), so a product
-        // is the same bits whatever the slips' alignment.
-        const int ns = ks_slices(n, nvec, bn, tk < 2 ? M->ring_slots[tk] : M->ks_slots);
+        const int ns = ks_slices(n, nvec, bn, M->ks_slots[tk]);
         CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)ne * ns));
         const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + bn - 1) / bn));
+        const bool v2 = gemv_vec2_ok(K, n) && gemv_vec2_ok(s, n);
         double *pp = M->part.as<double>();
-        unsigned *ep = M->err.as<unsigned>();
-        if (ring && tk == 0)
-            gemm_ks_dmma_ring_kernel<1, 32, 4><<<grid, 256, KsRing<1, 32, 4>::SMEM, st>>>(K, s, n, ns, nvec, pp, ep);
-        else if (ring)
-            gemm_ks_dmma_ring_kernel<2, 32, 4><<<grid, 256, KsRing<2, 32, 4>::SMEM, st>>>(K, s, n, ns, nvec, pp, ep);
-        else {
 #define EQD_KS(V, NT) gemm_ks_dmma_kernel<V, NT, (NT < 4 ? 32 : 16)><<<grid, 256, 0, st>>>(K, s, n, ns, nvec, pp)
-        if (tk == 0) EQD_KS(false, 1);          // 8-byte loads (the ring takes the rest)
-        else if (tk == 1) EQD_KS(false, 2);
-        else if (v2) EQD_KS(true, 4);
-        else EQD_KS(false, 4);
+        if (tk == 0) { if (v2) EQD_KS(true, 1); else EQD_KS(false, 1); }
+        else if (tk == 1) { if (v2) EQD_KS(true, 2); else EQD_KS(false, 2); }
+        else { if (v2) EQD_KS(true, 4); else EQD_KS(false, 4); }
 #undef EQD_KS
-        }
         gemv_reduce_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(M->part.as<double>(), n, ns, nvec, y);
     } else {
         const int nslice = gemv_slices(n);
@@ -2184,15 +2157,7 @@ extern "C" int eqd_kmat_gemv(eqd_kmat *M, const double *s, double *y, int32_t nv
     const int rc = kmat_apply(M, M->s.as<double>(), M->y.as<double>(), nvec, M->stream);
     if (rc) return rc;
     CUDA_OR_RETURN(cudaMemcpyAsync(y, M->y.p, bytes, cudaMemcpyDeviceToHost, M->stream));
-    unsigned derr = 0;
-    CUDA_OR_RETURN(cudaMemcpyAsync(&derr, M->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, M->stream));
     CUDA_OR_RETURN(cudaStreamSynchronize(M->stream));
-    if (derr) {
-        // A bounded wait of the K S gave up (this call's or an earlier
-        // device-entry call's): report it once.
-        CUDA_OR_RETURN(cudaMemset(M->err.p, 0, sizeof(unsigned)));
-        return fail(EQD_ERR_TIMEOUT, "a K S copy wait timed out; y is not valid");
-    }
     return EQD_OK;
 }
 

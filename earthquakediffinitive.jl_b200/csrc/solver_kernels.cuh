@@ -1007,136 +1007,6 @@ __global__ void __launch_bounds__(256, 2) gemm_ks_dmma_kernel(const double *__re
     }
 }
 
-// ---------------------------------------------------------------------------
-// The narrow K S tiles (16 or 32 vectors per CTA) stream K faster than the
-// tensor cores consume it, so they are bound by the bytes each CTA keeps in
-// flight. This form fills a ring of NS shared-memory stages with
-// cp.async.bulk copies completing on one mbarrier per stage: one thread
-// issues, per step, KB rows of the K tile (up to 1 KB each, into the same
-// 132-double rows) and one KB-column run of S per vector, and refills a stage
-// as soon as every warp has passed it, so NS - 1 steps are in flight while
-// one is multiplied. Same tiles, fragment layout, k order, slices and
-// partial-sum layout as gemm_ks_dmma_kernel, so the products are the same
-// bits. Requires 16-byte loads (n even; K, S 16-byte aligned). Rows past n
-// and vectors past nvec are not copied (their stale shared memory reaches
-// only output rows and vectors that are never stored); columns past the
-// slice's end are masked to zero in the fragments. Waits are bounded: on
-// expiry the CTA records DERR_MBAR_TIMEOUT in *err, waits (bounded) for the
-// copies it issued and returns.
-// ---------------------------------------------------------------------------
-template <int NT, int KB, int NS>
-struct KsRing {
-    static constexpr int BN = 16 * NT, BST = KB + 4;
-    static constexpr int A_ELEMS = KB * kDmmaAStride, B_ELEMS = BN * BST;
-    static constexpr int STAGE = A_ELEMS + B_ELEMS;  // doubles per stage (multiple of 2)
-    static constexpr int HEADER = 128;                // bytes: NS mbarriers + the dead flag
-    static constexpr size_t SMEM = HEADER + (size_t)NS * STAGE * sizeof(double);
-    static_assert(8 * NS + 4 <= HEADER, "ring header");
-};
-
-template <int NT, int KB, int NS>
-__global__ void __launch_bounds__(256, 1) gemm_ks_dmma_ring_kernel(const double *__restrict__ K,
-                                                                   const double *__restrict__ S, long long n,
-                                                                   int nslice, int nvec, double *__restrict__ part,
-                                                                   unsigned *__restrict__ err) {
-    using R = KsRing<NT, KB, NS>;
-    extern __shared__ __align__(128) unsigned char ks_smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(ks_smem);
-    volatile int *s_dead = reinterpret_cast<volatile int *>(ks_smem + 8 * NS);
-    double *ring = reinterpret_cast<double *>(ks_smem + R::HEADER);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int wm = warp & 3, wn = warp >> 2;
-    const long long row0 = (long long)blockIdx.x * kDmmaBM;
-    const int slice = blockIdx.y;
-    const int v0 = blockIdx.z * R::BN;
-    const long long c0 = dmma_slice_bound(n, slice, nslice), c1 = dmma_slice_bound(n, slice + 1, nslice);
-    const int nsteps = (int)((c1 - c0 + KB - 1) / KB);
-    const int rows = (int)min((long long)kDmmaBM, n - row0);
-    const int nv = min(R::BN, nvec - v0);
-
-    if (tid == 0) {
-        for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
-        *s_dead = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
-    // Step i's copies into stage i % NS (thread 0 only).
-    auto issue = [&](int i) {
-        const long long k0 = c0 + (long long)i * KB;
-        double *As = ring + (size_t)(i % NS) * R::STAGE;
-        double *Bs = As + R::A_ELEMS;
-        const int kn = (int)min((long long)KB, c1 - k0);
-        uint64_t *b = &bar[i % NS];
-        mbar_arrive_expect_tx(b, (unsigned)(kn * rows + nv * kn) * 8u);
-        for (int kk = 0; kk < kn; ++kk) bulk_g2s(As + kk * kDmmaAStride, K + (k0 + kk) * n + row0, rows * 8u, b);
-        for (int j = 0; j < nv; ++j) bulk_g2s(Bs + j * R::BST, S + (long long)(v0 + j) * n + k0, kn * 8u, b);
-    };
-    const int first = min(NS, nsteps);
-    if (tid == 0)
-        for (int i = 0; i < first; ++i) issue(i);
-    int issued = first, dead_at = -1;
-
-    double acc[4][NT][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    for (int i = 0; i < nsteps; ++i) {
-        const bool ok = mbar_wait_bounded(&bar[i % NS], (unsigned)(i / NS) & 1u, err);
-        if (!ok) *s_dead = 1;
-        if (ok) {
-            const long long k0 = c0 + (long long)i * KB;
-            const double *As = ring + (size_t)(i % NS) * R::STAGE;
-            const double *Bs = As + R::A_ELEMS;
-            const bool tail = k0 + KB > c1;
-#pragma unroll
-            for (int kq = 0; kq < KB / 4; ++kq) {
-                const bool live = !tail || k0 + kq * 4 + t < c1;
-                double a[4], b[NT];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) a[r] = live ? As[(kq * 4 + t) * kDmmaAStride + wm * 32 + r * 8 + g] : 0.0;
-#pragma unroll
-                for (int j = 0; j < NT; ++j) b[j] = live ? Bs[(wn * 8 * NT + j * 8 + g) * R::BST + kq * 4 + t] : 0.0;
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-#pragma unroll
-                    for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[r][j], a[r], b[j]);
-            }
-        }
-        __syncthreads();
-        if (*s_dead) {
-            dead_at = i;
-            break;
-        }
-        // Every warp has passed stage i % NS: refill it with step i + NS.
-        if (i + NS < nsteps) {
-            if (tid == 0) issue(i + NS);
-            issued = i + NS + 1;
-        }
-    }
-    if (dead_at >= 0) {
-        // Before the CTA's shared memory is released, wait (bounded) for
-        // every copy issued and not yet consumed.
-        if (tid == 0)
-            for (int q = dead_at; q < issued; ++q) mbar_wait_bounded(&bar[q % NS], (unsigned)(q / NS) & 1u, err);
-        __syncthreads();
-        return;
-    }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const long long row = row0 + wm * 32 + r * 8 + g;
-        if (row >= n) continue;
-#pragma unroll
-        for (int j = 0; j < NT; ++j)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int v = v0 + wn * 8 * NT + j * 8 + 2 * t + e;
-                if (v < nvec) part[((long long)v * nslice + slice) * n + row] = acc[r][j][e];
-            }
-    }
-}
-
 __global__ void gemv_reduce_kernel(const double *__restrict__ part, long long n, int nslice, int nvec,
                                    double *__restrict__ y) {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;

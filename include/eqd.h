@@ -244,9 +244,7 @@ int eqd_kmat_gemv(eqd_kmat *kmat, const double *s, double *y, int32_t nvec);
  * cudaStream_t, NULL = default stream) and returns without synchronizing.
  * Partial sums live in scratch owned by the kmat: calls on one kmat must be
  * serialised (one stream, or events), and the first call with a given n * nvec
- * may allocate it (make that call before any stream capture). The K S's
- * shared-memory copy waits are bounded; one that gives up is reported as
- * EQD_ERR_TIMEOUT by the next eqd_kmat_gemv call on the kmat. */
+ * may allocate it (make that call before any stream capture). */
 int eqd_kmat_gemv_device(eqd_kmat *kmat, const double *s_device, double *y_device, int32_t nvec, void *stream);
 int eqd_kmat_destroy(eqd_kmat *kmat);
 
