@@ -2125,6 +2125,9 @@ static int kmat_apply(eqd_kmat *M, const double *s, double *y, int nvec, cudaStr
     if (nvec >= kGemmMinVectors) {
         // Vector tile: 16, 32 or 64 vectors per CTA, the narrowest that holds nvec.
         const int tk = nvec <= 16 ? 0 : nvec <= 32 ? 1 : 2, bn = 16 << tk;
+        // The slice count depends only on n, nvec and the tile (the
+        // occupancy of the 16-byte-load instance on either load path), so a
+        // product is the same bits whatever the slips' alignment.
         const int ns = ks_slices(n, nvec, bn, M->ks_slots[tk]);
         CUDA_OR_RETURN(M->part.ensure(sizeof(double) * (size_t)ne * ns));
         const dim3 grid((unsigned)((n + kDmmaBM - 1) / kDmmaBM), (unsigned)ns, (unsigned)((nvec + bn - 1) / bn));

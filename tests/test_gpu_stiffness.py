@@ -208,6 +208,32 @@ def test_kmat_gemv_device(eqd, n, nvec):
     assert abs(Yd - K @ S).max() <= 1e-13 * scale
 
 
+@pytest.mark.parametrize("n, nvec", [(4356, 8), (2178, 16), (4356, 30), (578, 64)])
+def test_ks_load_paths_same_bits(eqd, n, nvec):
+    """The K S with 16-byte loads (slips 16-byte aligned) and with 8-byte
+    loads (the same slips 8 bytes into a buffer) runs the same tiles, slices
+    and k order: the same bits."""
+    import torch
+    rng = np.random.default_rng(n * nvec)
+    K = rng.standard_normal((n, n))
+    S = rng.standard_normal((nvec, n))
+    M = eqd.KMatrix(K)
+    buf = torch.zeros(nvec * n + 1, dtype=torch.float64, device="cuda")
+    s_odd = buf[1:].view(nvec, n)
+    s_odd.copy_(torch.from_numpy(S))
+    s_al = torch.from_numpy(S).cuda()
+    assert s_odd.data_ptr() % 16 == 8 and s_al.data_ptr() % 16 == 0
+    y_al, y_odd = torch.empty_like(s_al), torch.empty_like(s_al)
+    st = torch.cuda.current_stream()
+    M.gemv_device(s_al, y_al, stream=st)
+    M.gemv_device(s_odd, y_odd, stream=st)
+    st.synchronize()
+    M.close()
+    assert torch.equal(y_al, y_odd)
+    Y = y_al.cpu().numpy()
+    assert abs(Y - S @ K.T).max() <= 1e-13 * abs(S).dot(abs(K).T).max()
+
+
 def test_gemv(eqd):
     rng = np.random.default_rng(0)
     n = 578
