@@ -163,7 +163,8 @@ def test_bp8_dz100_model(eqd):
     assert rel(K, K_ref) < K_TOL
 
 
-@pytest.mark.parametrize("n, nvec", [(578, 8), (1155, 64), (2178, 70), (1155, 12), (1155, 20), (4356, 24), (4356, 130)])
+@pytest.mark.parametrize("n, nvec", [(578, 8), (1155, 64), (2178, 70), (1155, 12), (1155, 20), (4356, 24), (4356, 130),
+                                     (6, 5), (7, 40), (130, 3)])
 def test_batched_ks(eqd, n, nvec):
     """y = K S for many slip vectors (the blocked K S on the FP64 tensor
     cores: 16-, 32- and 64-vector tiles, odd n on 8-byte loads, more than 64
